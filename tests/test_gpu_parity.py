@@ -1,0 +1,135 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+Topology (ids, ptr, vals, counts) must be bit-exact.  Positions must be
+bit-exact too: the CUDA kernels evaluate the reference's formulas in the
+serialized-atomic order the oracle restates, with IEEE float and no FMA
+contraction (tolerance 0 ulp; NaN == NaN).  Against FP64 the bound is
+1e-6 of the input's bounding-box diagonal."""
+import numpy as np
+import pytest
+
+import oracle
+from slak_b200 import api, meshgen
+from slak_b200.mesh import LAK, QUAD, SLAK
+
+from meshes import small_set, open_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits_equal(a, b):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    same = a.view(np.uint32) == b.view(np.uint32)
+    return bool((same | (np.isnan(a) & np.isnan(b))).all())
+
+
+def _check(mesh, levels, scheme, flags=0):
+    ref = oracle.subdivide(mesh, levels, scheme, fp64=True)
+    got = api.subdivide(mesh, levels, scheme, flags)
+    assert (got.nfaces, got.nnz, got.nverts) == (ref.nfaces, ref.nnz, ref.nverts)
+    assert got.type == QUAD and got.is_reduced == ref.is_reduced and got.max_face_order == ref.max_face_order
+    assert np.array_equal(got.ids, ref.ids)
+    if scheme == LAK:
+        assert np.array_equal(got.ptr, ref.ptr) and np.array_equal(got.vals, ref.vals)
+    else:
+        assert got.ptr is None and got.vals is None
+    return got, ref
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("case", small_set(), ids=lambda c: c[0])
+def test_small_meshes_bit_exact(case, scheme):
+    name, mesh, levels = case
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    got, ref = _check(mesh, levels, scheme)
+    assert _bits_equal(got.verts, ref.verts)
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name,levels", [("torus32", 3), ("icosphere", 4), ("cylinder", 4)])
+def test_workloads_bit_exact_and_fp64(name, levels, scheme):
+    w = meshgen.workload(name)
+    got, ref = _check(w.mesh, levels, scheme)
+    assert _bits_equal(got.verts, ref.verts)
+    err = np.abs(got.verts[:, :3].astype(np.float64) - ref.verts64[:, :3]).max() / w.mesh.bbox_diag()
+    assert err <= 1e-6, err
+
+
+def test_mixed_torus_reduced_size():
+    m = meshgen.mixed_torus(96, 80, 0.05, 0.03, 0.005, seed=21)
+    for scheme in (SLAK, LAK):
+        got, ref = _check(m, 3, scheme)
+        assert _bits_equal(got.verts, ref.verts)
+
+
+def test_compensated_is_closer_to_fp64():
+    w = meshgen.workload("cylinder")
+    ref = oracle.subdivide(w.mesh, 5, SLAK, fp64=True)
+    plain = api.subdivide(w.mesh, 5, SLAK)
+    comp = api.subdivide(w.mesh, 5, SLAK, api._abi.PLAN_COMPENSATED)
+    assert np.array_equal(comp.ids, ref.ids)
+    d = w.mesh.bbox_diag()
+    e_plain = np.abs(plain.verts[:, :3] - ref.verts64[:, :3]).max() / d
+    e_comp = np.abs(comp.verts[:, :3] - ref.verts64[:, :3]).max() / d
+    assert e_comp <= e_plain and e_comp <= 1e-6
+
+
+def test_plan_graph_replay_identical():
+    import torch
+    m = meshgen.workload("icosphere").mesh
+    dm = api.DeviceMesh.from_host(m)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        plan = api.Plan(dm, 3, SLAK, api._abi.PLAN_GRAPH, stream=s)
+        outs = []
+        for _ in range(3):
+            plan.execute(s)
+            plan.check(s)
+            o = plan.output()
+            outs.append((o.ids.cpu().numpy().copy(), o.verts.cpu().numpy().copy()))
+    ref = oracle.subdivide(m, 3, SLAK)
+    for ids, verts in outs:
+        assert np.array_equal(ids, ref.ids) and _bits_equal(verts.reshape(-1, 4), ref.verts)
+    assert plan.launches > 0
+    stats = plan.level_stats()
+    assert len(stats) == 3 and stats[-1]["out_faces"] == ref.nfaces
+    plan.close()
+
+
+@pytest.mark.parametrize("cls,scheme", [(api.CatmullClark, SLAK), (api.LAKCatmullClark, LAK)])
+def test_reference_shaped_entry_points(cls, scheme):
+    m = meshgen.workload("icosphere").mesh
+    cm = api.DeviceMesh.from_host(m)
+    rm = api.DeviceMesh()
+    cls.subdivideIteratively(cm, rm, 2)
+    ref = oracle.subdivide(m, 2, scheme)
+    h = rm.to_host()
+    assert np.array_equal(h.ids, ref.ids) and _bits_equal(h.verts, ref.verts)
+    assert h.nverts == ref.nverts and h.nfaces == ref.nfaces
+    # input untouched
+    assert np.array_equal(cm.ids.cpu().numpy(), m.ids)
+
+
+def test_quad_input_level_zero_leaves_output_untouched():
+    m = meshgen.torus(8, 8)
+    cm = api.DeviceMesh.from_host(m)
+    rm = api.DeviceMesh()
+    api.CatmullClark.subdivideIteratively(cm, rm, 0)
+    assert rm.ids is None and rm.nfaces == 0
+
+
+def test_bad_meshes_rejected():
+    m = meshgen.torus(6, 6)
+    bad = m.copy()
+    bad.ids = bad.ids.copy()
+    bad.ids[5] = m.nverts + 3                  # index out of range
+    with pytest.raises(api._abi.SlakError) as e:
+        api.subdivide(bad, 1, SLAK)
+    assert e.value.code == 4
+    bad = m.copy()
+    bad.ids = bad.ids.copy()
+    bad.ids[0:4] = bad.ids[4:8]               # duplicated face: non-manifold edges
+    with pytest.raises(api._abi.SlakError):
+        api.subdivide(bad, 1, SLAK)
