@@ -251,9 +251,9 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
         out_ids.copy_(api.device_view(cout.ids, (cout.nnz,), "<i4"), non_blocking=True)
         out_verts.copy_(api.device_view(cout.verts, (4 * cout.nverts,), "<f4"), non_blocking=True)
         torch.cuda.synchronize()
+        faces = cout.nfaces
         lib.slak_mesh_free(ctypes.byref(cout))
         dt = time.perf_counter() - t0
-        faces = cout.nfaces
         if i >= args.warmup:
             times.append(dt)
     t = _max_over_ranks(dist, statistics.mean(times))

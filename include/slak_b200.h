@@ -63,6 +63,12 @@ const char* slak_status_string(int status);
 /* SLAK_B200_ABI_VERSION of the loaded library. */
 int slak_abi_version(void);
 
+/* Detail of the last failure on the calling thread (the CUDA error text and,
+ * with SLAK_DEBUG_SYNC=1 set when the plan was created, the kernel that
+ * failed); empty if none.  The reference printed CUDA errors before throwing
+ * (LibInclude/cuda_host_helpers.h:34-41). */
+const char* slak_last_error_detail(void);
+
 /*
  * Replaces CatmullClark::subdivideIteratively (LibSource/device/CatmullClarkImpl.cu:457-515)
  * and LAKCatmullClark::subdivideIteratively (LibSource/device/LAKCatmullClarkImpl.cu:512-571);

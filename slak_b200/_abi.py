@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: 
 PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED = 1, 2, 4
 
 # every symbol include/slak_b200.h declares
-EXPORTS = ["slak_status_string", "slak_abi_version", "slak_subdivide", "slak_mesh_free", "slak_plan_create",
+EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free", "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_destroy"]
 
@@ -40,7 +40,11 @@ class LevelStats(ctypes.Structure):
 class SlakError(RuntimeError):
     def __init__(self, code: int, what: str = ""):
         self.code = code
-        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)} ({status_string(code)})")
+        try:
+            detail = lib().slak_last_error_detail().decode()
+        except Exception:
+            detail = ""
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)} ({status_string(code)}) {detail}")
 
 
 _lib = None
@@ -57,6 +61,7 @@ def lib():
         L.slak_status_string.argtypes = [I]
         L.slak_status_string.restype = ctypes.c_char_p
         L.slak_abi_version.restype = I
+        L.slak_last_error_detail.restype = ctypes.c_char_p
         L.slak_subdivide.argtypes = [P, P, I, I, V]
         L.slak_mesh_free.argtypes = [P]
         L.slak_plan_create.argtypes = [P, I, I, I, V, ctypes.POINTER(V)]

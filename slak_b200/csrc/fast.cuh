@@ -1,0 +1,378 @@
+// fast.cuh -- closed-form refinement of an already refined quad mesh.
+//
+// Let P be a closed quad mesh (N1 corners, V1 vertices, F1 = N1/4 faces,
+// E1 = N1/2 edges) and C = refine(P) the level being refined now: quad x of C
+// is corner x of P, corner 4x+k of C is corner k of that quad, and C's
+// vertices are [V1 old | F1 face points | E1 edge points].  Everything the
+// general path rebuilds with atomics, sorting and searching is then known in
+// closed form from P's adjacency state:
+//
+//   sptr1 / sc1   P's vertex columns (corners of each vertex, corner order)
+//   slot1         inverse of sc1 (corner -> its slot)
+//   tw1           twin half-edge of each corner of P
+//   t1            slot1[tw1[prev(x)]] (SLAK)
+//   H1            P's edges in the scheme's numbering: (min->max, max->min)
+//
+// C's adjacency: vertex v < V1 keeps its column with corners 4x (x in
+// column order), face point V1+g owns corners 4x+2 of g's four corners,
+// edge point V1+F1+e owns the sorted corners {4h+1, 4h'+1, 4nh+3, 4nh'+3} of
+// e's half-edges (h, h').  C's edge ids (serialized atomics of the reference):
+//   SLAK  eid(4x+0) = slot1(x), eid(4x+1) = N1 + next(x), eid(4x+2) = N1 + x,
+//         eid(4x+3) = slot1(tw1(prev x))            [owners ranked by (tail, corner)]
+//   LAK   edges around edge point e are 4e + {lower end, higher end,
+//         lower face point, higher face point}      [ascending (max, min)]
+//
+// Three kernels per level write every output exactly once, in contiguous runs:
+//   k_g1  per face of P (16 threads, one per corner of C): C's refined quads,
+//         face points of C, vertex points of the face points of P, SLAK edge
+//         points N1+x, and the next level's per-corner state
+//   k_g2  per edge of P: vertex points of the edge points of P, LAK edge points
+//   k_g3  per vertex of P: vertex points of P's vertices, SLAK edge points slot1(x)
+// The float arithmetic and its order are exactly the general path's (and the
+// reference's serialized order), so both paths are bit-identical.
+#pragma once
+
+#include "common.cuh"
+
+namespace slak {
+
+__device__ __forceinline__ int qnext(int x) { return (x & ~3) | ((x + 1) & 3); }
+__device__ __forceinline__ int qprev(int x) { return (x & ~3) | ((x + 3) & 3); }
+
+// P's adjacency state (read) / C's (written when another level follows)
+struct QState {
+    int* sptr;
+    int* sc;
+    int* slot;
+    int* tw;
+    int* t;
+    int2* H;
+};
+
+struct FastDims {
+    int N1, V1, F1, E1;    // P
+    int V, N;              // C (F = N1, E = 2 N1)
+};
+
+__device__ __forceinline__ float4 shfl4(float4 v, int src)
+{
+    return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                       __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+__device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
+{
+    return make_float4(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
+                       __shfl_xor_sync(0xffffffffu, v.z, m), __shfl_xor_sync(0xffffffffu, v.w, m));
+}
+
+// rank of corner `a` among the four corners of an edge point
+__device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a) + (c < a) + (d < a); }
+
+// ---------------------------------------------------------------------------------------------
+// G1: one thread per corner y of C; the 16 corners of a face g of P are 16 consecutive lanes.
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
+                                               QState p, QState c, int4* __restrict__ out_ids,
+                                               float* __restrict__ R)
+{
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = y < d.N;
+    const int lane = threadIdx.x & 31;
+    const int qb = lane & ~3;            // lane of corner 0 of my quad
+    const int gb = lane & ~15;           // lane of corner 0 of my group's quad 0
+    const int x = y >> 2, k = y & 3, q = x & 3;
+    const int VF1 = d.V1 + d.F1;
+    const int VFc = d.V + d.N1;          // C: V + F
+
+    const int vid = valid ? __ldg(ids + y) : 0;
+    const float4 pos = valid ? ldg4(P, vid) : f4_zero();
+    int tw1x = 0, s1 = 0, t1x = 0;
+    if (valid && (LAK || STATE)) tw1x = __ldg(p.tw + x);
+    if (valid && !LAK) { s1 = __ldg(p.slot + x); t1x = __ldg(p.t + x); }
+
+    // values from the other corners / quads of the group
+    const int lq_next = gb | (((q + 1) & 3) << 2), lq_prev = gb | (((q + 3) & 3) << 2);
+    const int v1 = __shfl_sync(0xffffffffu, vid, qb + 1);              // e_out(x) id
+    const int v3 = __shfl_sync(0xffffffffu, vid, qb + 3);              // e_in(x) id
+    const int tw1_px = __shfl_sync(0xffffffffu, tw1x, lq_prev);        // tw1(prev x)
+    const int eidp_x = v1 - VF1, eidp_px = v3 - VF1;                   // P's edge ids of x, prev(x)
+
+    int eid;
+    if (!LAK) {
+        eid = k == 0 ? s1 : k == 1 ? d.N1 + qnext(x) : k == 2 ? d.N1 + x : t1x;
+    } else {
+        const int vx = __shfl_sync(0xffffffffu, vid, qb);
+        const int vnx = __shfl_sync(0xffffffffu, vid, lq_next);
+        const int vpx = __shfl_sync(0xffffffffu, vid, lq_prev);
+        const int fx = x >> 2;
+        eid = k == 0 ? 4 * eidp_x + (vx > vnx)
+            : k == 1 ? 4 * eidp_x + 2 + (fx > (tw1x >> 2))
+            : k == 2 ? 4 * eidp_px + 2 + (fx > (tw1_px >> 2))
+                     : 4 * eidp_px + (vx > vpx);
+    }
+    const int ein = __shfl_sync(0xffffffffu, eid, qb + ((k + 3) & 3));
+    if (valid) __stcs(out_ids + y, make_int4(vid, VFc + eid, d.V + x, VFc + ein));
+
+    // face point of quad x
+    float4 fp;
+    if (!LAK) {
+        float4 a = f4_add(pos, shfl4_xor(pos, 2));
+        fp = f4_mul(f4_add(a, shfl4_xor(a, 1)), 0.25f);
+    } else {
+        float4 acc = f4_add(f4_zero(), shfl4(pos, qb));
+        acc = f4_add(acc, shfl4(pos, qb + 1));
+        acc = f4_add(acc, shfl4(pos, qb + 2));
+        acc = f4_add(acc, shfl4(pos, qb + 3));
+        fp = f4_div_z(acc, 4.0f);
+    }
+    if (valid && k == 0) st4(R, (int64_t)d.V + x, fp);
+
+    // vertex point of the face point V1 + g (corners 4x+2 of the group's quads, n = 4)
+    {
+        float4 nb[4], fq[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            nb[j] = shfl4(pos, gb | (j << 2) | (LAK ? 1 : 3));   // SLAK: e_in(x) positions; LAK: tails e_out(x)
+            fq[j] = shfl4(fp, gb | (j << 2));
+        }
+        const float4 pf = shfl4(pos, gb | 2);
+        float4 yv;
+        if (!LAK) {
+            float4 acc = f4_zero();
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc = f4_add(acc, nb[j]);
+            yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(pf, 2.0f), 4.0f));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) yv = f4_add(yv, f4_div(fq[j], 16.0f));
+        } else {
+            int tid[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) tid[j] = __shfl_sync(0xffffffffu, vid, gb | (j << 2) | 1);
+            float4 acc = f4_zero();
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc = f4_add(acc, fq[j]);
+            // tails in ascending vertex id
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    int rk = 0;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) rk += tid[i] < tid[j];
+                    if (rk == r) acc = f4_add(acc, nb[j]);
+                }
+            }
+            yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(pf, 2.0f)), 4.0f);
+        }
+        if (valid && (lane & 15) == 0) st4(R, (int64_t)d.V1 + (x >> 2), yv);
+    }
+
+    // SLAK edge point N1 + x: half-edges 4x+2 (tail f, quad x) and 4 prev(x)+1 (tail e_in(x), quad prev x)
+    if (!LAK) {
+        const float4 fprev = shfl4(fp, lq_prev);
+        const float4 pf = shfl4(pos, qb + 2), pin = shfl4(pos, qb + 3);
+        if (valid && k == 2) {
+            float4 ta = f4_mul(f4_add(pf, fp), 0.25f);
+            float4 tb = f4_mul(f4_add(pin, fprev), 0.25f);
+            st4_cs(R, (int64_t)VFc + d.N1 + x, f4_add(f4_add(f4_zero(), ta), tb));
+        }
+    }
+
+    if (STATE && valid) {
+        // C's slot / twin / t for corner y
+        const int px = qprev(x), nxx = qnext(x);
+        const int ntw = qnext(tw1x), ntwp = qnext(tw1_px);
+        // edge of P through x: corners A=4x+1, B=4tw1x+1, Cc=4nxx+3, D=4ntw+3
+        const int A = 4 * x + 1, B = 4 * tw1x + 1, Cc = 4 * nxx + 3, D = 4 * ntw + 3;
+        // edge of P through prev(x): A'=4px+1, B'=4tw1_px+1, C'=4x+3, D'=4ntwp+3
+        const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
+        const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
+        int sl, tw;
+        if (k == 0) { sl = s1; tw = 4 * ntw + 3; }
+        else if (k == 1) { sl = base_x + rank4(A, B, Cc, D); tw = 4 * nxx + 2; }
+        else if (k == 2) { sl = d.N1 + x; tw = 4 * px + 1; }
+        else { sl = base_px + rank4(C2, A2, B2, D2); tw = 4 * tw1_px; }
+        c.slot[y] = sl;
+        c.tw[y] = tw;
+        if (!LAK) {
+            int tt = k == 0 ? t1x
+                   : k == 1 ? base_x + rank4(D, A, B, Cc)
+                   : k == 2 ? d.N1 + nxx
+                            : base_px + rank4(A2, B2, C2, D2);
+            c.t[y] = tt;
+        }
+        if (k == 2) {
+            c.sc[d.N1 + x] = y;                                   // face point column
+            if (!LAK) c.H[d.N1 + x] = make_int2(y, 4 * px + 1);   // SLAK edge N1 + x
+        }
+        if ((lane & 15) == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + 4 * (x >> 2);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// G2: one thread per edge e of P, half-edges (h, h2) = H1[e] (min->max, max->min of P)
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
+                                               QState p, QState c, float* __restrict__ R)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d.E1) return;
+    const int2 hh = __ldg(p.H + e);
+    const int h = hh.x, h2 = hh.y, nh = qnext(h), nh2 = qnext(h2);
+    const int ve = d.V1 + d.F1 + e;
+    const int v = __ldg(ids + 4 * h), u = __ldg(ids + 4 * h2);
+    const int fh = d.V1 + (h >> 2), fh2 = d.V1 + (h2 >> 2);
+    const float4 Pv = ldg4(P, v), Pu = ldg4(P, u), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2), Pe = ldg4(P, ve);
+    const float* FP = R + 4 * (int64_t)d.V;
+    const float4 Fh = ldg4(FP, h), Fh2 = ldg4(FP, h2), Fnh = ldg4(FP, nh), Fnh2 = ldg4(FP, nh2);
+    // corners of the edge point: A=4h+1 (nbr fh, face h), B=4h2+1 (fh2, h2), C=4nh+3 (u, nh), D=4nh2+3 (v, nh2)
+    const int A = 4 * h + 1, B = 4 * h2 + 1, Cc = 4 * nh + 3, D = 4 * nh2 + 3;
+    const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D), rD = rank4(D, A, B, Cc);
+    float4 nb[4], fq[4];
+    int co[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        nb[r] = rA == r ? Pf : rB == r ? Pf2 : rC == r ? Pu : Pv;
+        fq[r] = rA == r ? Fh : rB == r ? Fh2 : rC == r ? Fnh : Fnh2;
+        co[r] = rA == r ? A : rB == r ? B : rC == r ? Cc : D;
+    }
+    float4 yv;
+    if (!LAK) {
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = f4_add(acc, nb[r]);
+        yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(Pe, 2.0f), 4.0f));
+#pragma unroll
+        for (int r = 0; r < 4; ++r) yv = f4_add(yv, f4_div(fq[r], 16.0f));
+    } else {
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = f4_add(acc, fq[r]);
+        // tails {v, u, fh, fh2} in ascending id: v,u < V1 <= fh, fh2
+        const bool vu = v < u, ff = fh < fh2;
+        acc = f4_add(acc, vu ? Pv : Pu);
+        acc = f4_add(acc, vu ? Pu : Pv);
+        acc = f4_add(acc, ff ? Pf : Pf2);
+        acc = f4_add(acc, ff ? Pf2 : Pf);
+        yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(Pe, 2.0f)), 4.0f);
+    }
+    st4_cs(R, ve, yv);
+
+    if (LAK) {
+        // edges 4e + {lower end, higher end, lower face point, higher face point}
+        const float4 Ev = f4_mul(f4_add(f4_add(f4_add(Pv, Pe), Fh), Fnh2), 0.25f);
+        const float4 Eu = f4_mul(f4_add(f4_add(f4_add(Pu, Pe), Fh2), Fnh), 0.25f);
+        const float4 Ef = f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f);
+        const float4 Ef2 = f4_mul(f4_add(f4_add(f4_add(Pf2, Pe), Fnh2), Fh2), 0.25f);
+        const bool vu = v < u, ff = fh < fh2;
+        const int64_t base = (int64_t)d.V + d.N1 + 4 * (int64_t)e;
+        st4_cs(R, base + 0, vu ? Ev : Eu);
+        st4_cs(R, base + 1, vu ? Eu : Ev);
+        st4_cs(R, base + 2, ff ? Ef : Ef2);
+        st4_cs(R, base + 3, ff ? Ef2 : Ef);
+        if (STATE) {
+            const int2 Hv = make_int2(4 * h, 4 * nh2 + 3), Hu = make_int2(4 * h2, 4 * nh + 3);
+            const int2 Hf = make_int2(4 * nh + 2, 4 * h + 1), Hf2 = make_int2(4 * nh2 + 2, 4 * h2 + 1);
+            int2* H = c.H + 4 * (int64_t)e;
+            H[0] = vu ? Hv : Hu;
+            H[1] = vu ? Hu : Hv;
+            H[2] = ff ? Hf : Hf2;
+            H[3] = ff ? Hf2 : Hf;
+        }
+    }
+    if (STATE) {
+        reinterpret_cast<int4*>(c.sc + 2 * (int64_t)d.N1)[e] = make_int4(co[0], co[1], co[2], co[3]);
+        c.sptr[ve] = 2 * d.N1 + 4 * e;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// G3: one thread per vertex v of P (its column of corners x, each giving C's corner 4x)
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
+                                               QState p, QState c, float* __restrict__ R, int compensated)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= d.V1) {
+        if (STATE && v == d.V1) c.sptr[d.V] = d.N;
+        return;
+    }
+    const int b = __ldg(p.sptr + v), e = __ldg(p.sptr + v + 1), n = e - b;
+    const float* FP = R + 4 * (int64_t)d.V;
+    const float4 Pv = ldg4(P, v);
+    const float nn = (float)(n * n);
+    const int64_t EPb = (int64_t)d.V + d.N1;       // C's edge points start at V + F
+    float4 yv;
+    if (!LAK) {
+        if (!compensated || n <= 4) {
+            float4 acc = f4_zero();
+            for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
+            yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
+            for (int s = b; s < e; ++s) yv = f4_add(yv, f4_div(ldg4(FP, __ldg(p.sc + s)), nn));
+        } else {
+            float4 sh = f4_zero(), sl = f4_zero();
+            for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
+            for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, __ldg(p.sc + s)));
+            yv = vp_finish(sh, sl, Pv, n);
+        }
+        // edge points of C's edges {v, e_out(x)}: ids slot1(x) = s
+        for (int s = b; s < e; ++s) {
+            const int x = __ldg(p.sc + s);
+            const int tw = __ldg(p.tw + x);
+            const int eo = __ldg(ids + 4 * x + 1);
+            float4 ta = f4_mul(f4_add(Pv, ldg4(FP, x)), 0.25f);
+            float4 tb = f4_mul(f4_add(ldg4(P, eo), ldg4(FP, qnext(tw))), 0.25f);
+            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), tb));
+            if (STATE) c.H[s] = make_int2(4 * x, 4 * qnext(tw) + 3);
+        }
+    } else {
+        // face points in column order, then the tails e_in(x) in ascending id
+        float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
+        const bool comp = compensated && n > 4;
+        for (int s = b; s < e; ++s) {
+            float4 f = ldg4(FP, __ldg(p.sc + s));
+            if (comp) dd_acc(sh, sl, f); else acc = f4_add(acc, f);
+        }
+        int last = -1;
+        while (true) {
+            int xm = INT32_MAX;
+            for (int s = b; s < e; ++s) {
+                int ti = __ldg(ids + 4 * __ldg(p.sc + s) + 3);
+                if (ti > last && ti < xm) xm = ti;
+            }
+            if (xm == INT32_MAX) break;
+            if (comp) dd_acc(sh, sl, ldg4(P, xm)); else acc = f4_add(acc, ldg4(P, xm));
+            last = xm;
+        }
+        if (comp) yv = vp_finish(sh, sl, Pv, n);
+        else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
+    }
+    st4(R, v, yv);
+    if (STATE) {
+        c.sptr[v] = b;
+        for (int s = b; s < e; ++s) c.sc[s] = 4 * __ldg(p.sc + s);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// State of a quad level built by the general path: corner -> slot, corner -> twin, t (SLAK)
+__global__ void k_export_state(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                               const int* __restrict__ stw, int* __restrict__ slot, int* __restrict__ tw)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    for (int s = sptr[v]; s < sptr[v + 1]; ++s) {
+        int c = sc[s];
+        slot[c] = s;
+        tw[c] = stw[s];
+    }
+}
+
+__global__ void k_export_t(int N, const int* __restrict__ slot, const int* __restrict__ tw, int* __restrict__ t)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= N) return;
+    t[x] = slot[tw[qprev(x)]];
+}
+
+}  // namespace slak

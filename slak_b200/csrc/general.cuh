@@ -191,7 +191,7 @@ __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int*
     const int VF = V + F;
     int4 q = make_int4(__ldg(ids + c), VF + __ldg(eid + c), V + fc.face(c), VF + __ldg(eid + fc.prev(c)));
     __stcs(out_ids + c, q);
-    if (LAK) {
+    if (LAK && out_vals != nullptr) {          // only the final level stores ptr / vals
         __stcs(out_vals + c, make_int4(1, 2, 3, 4));
         out_ptr[c] = 4 * c;
         if (c == N - 1) out_ptr[N] = 4 * N;

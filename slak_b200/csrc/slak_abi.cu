@@ -12,11 +12,14 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <cstdlib>
 #include <new>
 #include <vector>
 
 #include "common.cuh"
 #include "general.cuh"
+#include "fast.cuh"
 #include "scan.cuh"
 
 using namespace slak;
@@ -28,6 +31,10 @@ struct Level {
     int64_t Fo = 0, Vo = 0, No = 0;
     bool quad = true;       // implicit 4-corner faces
     bool poly_fn = false;   // the reference's first-level (polygon) functions
+    bool fast = false;      // closed-form refinement from the parent level's state
+    bool export_state = false;   // general level whose state feeds a fast level
+    bool make_state = false;     // fast level whose state feeds the next fast level
+    QState in_state{}, out_state{};
     const int* ptr = nullptr;
     const int* ids = nullptr;
     const float* verts = nullptr;
@@ -42,6 +49,7 @@ struct Scratch {
         *sprevc = nullptr, *stw = nullptr, *sflag = nullptr, *eid = nullptr, *ecnt = nullptr, *eptr = nullptr,
         *tmp = nullptr;
     int2* H = nullptr;
+    int *xslot = nullptr, *xtw = nullptr, *xt = nullptr;   // state export of a general quad level
 };
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -58,6 +66,30 @@ struct Carver {
         T* p = dry ? nullptr : reinterpret_cast<T*>(base + off);
         off += bytes;
         return p;
+    }
+};
+
+// Launch bookkeeping: counts launches and, in debug mode (SLAK_DEBUG_SYNC=1 in
+// the environment when the plan is created), synchronises after every launch
+// and records which kernel failed.
+thread_local std::string g_detail;
+
+struct Lc {
+    cudaStream_t s;
+    int64_t* nl;
+    bool debug;
+    int level;
+    int err = 0;
+    void after(const char* name, int n = 1)
+    {
+        *nl += n;
+        if (!debug || err) return;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            err = e == cudaErrorMemoryAllocation ? SLAK_ERR_OOM : SLAK_ERR_CUDA;
+            g_detail = std::string(name) + " (level " + std::to_string(level) + "): " + cudaGetErrorString(e);
+        }
     }
 };
 
@@ -86,11 +118,13 @@ struct slak_plan {
     DevStatus* h_st = nullptr;       // pinned
     int64_t maxN = 0, maxV = 0, maxE = 0;
     bool any_poly = false;
+    QState qs[2]{};
     // graph
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t gstream = nullptr;
     int64_t launches = 0;
     int executed = 0;
+    bool debug = false;
 };
 
 namespace {
@@ -114,21 +148,41 @@ void carve_scratch(Carver& cv, Scratch& s, int64_t N, int64_t V, int64_t E, bool
     s.H = cv.take<int2>(E);
 }
 
+void carve_export(Carver& cv, Scratch& s, int64_t N)
+{
+    s.xslot = cv.take<int>(N);
+    s.xtw = cv.take<int>(N);
+    s.xt = cv.take<int>(N);
+}
+
+void carve_state(Carver& cv, QState& q, int64_t N, int64_t V, int64_t E)
+{
+    q.sptr = cv.take<int>(V + 1);
+    q.sc = cv.take<int>(N);
+    q.slot = cv.take<int>(N);
+    q.tw = cv.take<int>(N);
+    q.t = cv.take<int>(N);
+    q.H = cv.take<int2>(E);
+}
+
 // Topology of a level up to the edge-offset scan (needs no output buffers).
-void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus* st, cudaStream_t str,
-                       int64_t* nl)
+void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus* st, Lc& lc)
 {
     const int F = (int)L.F, V = (int)L.V, N = (int)L.N;
+    cudaStream_t str = lc.s;
     if (!L.quad) {
         cudaMemsetAsync(s.cface, 0, sizeof(int) * (size_t)N, str);
         k_face_map<<<grid_for(F), kBlock, 0, str>>>(L.ptr, F, N, s.cface, st);
-        ++*nl;
+        lc.after("k_face_map");
     }
     cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
     k_valence<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.cnt, st);
-    scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, nl);
+    lc.after("k_valence");
+    int64_t dummy = 0;
+    scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, &dummy);
+    lc.after("scan(valence)", 3);
     k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sc);
-    *nl += 2;
+    lc.after("k_bucket");
     int* bcount = &st->bcount[li];
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
@@ -137,14 +191,25 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
         Faces<false> fc{L.ptr, s.cface};
         k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc);
     }
+    lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
         k_edges<true><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
                                                         s.ecnt, bcount, st);
     else
         k_edges<false><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
                                                          s.ecnt, bcount, st);
-    scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, nl);
-    *nl += 2;
+    lc.after("k_edges");
+    scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, &dummy);
+    lc.after("scan(edges)", 3);
+}
+
+__global__ void k_quad_ptr_vals(int N, int* __restrict__ ptr, int4* __restrict__ vals)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    __stcs(vals + c, make_int4(1, 2, 3, 4));
+    ptr[c] = 4 * c;
+    if (c == N - 1) ptr[N] = 4 * N;
 }
 
 __global__ void k_check_level(const int* eptr, int V, const int* bcount, int E, int B, DevStatus* st, int li)
@@ -153,17 +218,18 @@ __global__ void k_check_level(const int* eptr, int V, const int* bcount, int E, 
 }
 
 template <bool QUAD>
-void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevStatus* st, cudaStream_t str,
-                 int64_t* nl)
+void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevStatus* st, Lc& lc)
 {
     const int F = (int)L.F, V = (int)L.V, N = (int)L.N, E = (int)L.E;
     const bool lak = scheme == SLAK_SCHEME_LAK;
+    cudaStream_t str = lc.s;
     Faces<QUAD> fc{L.ptr, s.cface};
     if (lak)
         k_eids_lak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
                                                      s.H, st);
     else
         k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st);
+    lc.after("k_eids");
     if (lak)
         k_refine<QUAD, true><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
                                                               reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
@@ -171,6 +237,7 @@ void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevSt
     else
         k_refine<QUAD, false><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
                                                                reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr);
+    lc.after("k_refine");
     float* R = L.o_verts;
     float* FPo = R + 4 * (size_t)V;
     float* EPo = R + 4 * ((size_t)V + (size_t)F);
@@ -180,10 +247,12 @@ void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevSt
         k_fp_seq<QUAD, true><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
     else
         k_fp_seq<QUAD, false><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
+    lc.after("k_fp");
     if (lak)
         k_ep<QUAD, true><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
     else
         k_ep<QUAD, false><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+    lc.after("k_ep");
     const int bnd = L.B > 0;
     if (lak)
         k_vp_lak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
@@ -191,25 +260,75 @@ void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevSt
     else
         k_vp_slak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
                                                          L.verts, FPo, R, compensated);
-    *nl += 6;
+    lc.after("k_vp");
+}
+
+// One fast level: C = L (refined from its parent level Pl, whose state is L.in_state).
+template <bool LAK, bool STATE>
+void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
+{
+    FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N};
+    cudaStream_t str = lc.s;
+    k_g1<LAK, STATE><<<grid_for(L.N), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
+                                                         reinterpret_cast<int4*>(L.o_ids), L.o_verts);
+    lc.after("k_g1");
+    k_g2<LAK, STATE><<<grid_for(Pl.E), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+    lc.after("k_g2");
+    k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
+                                                             L.o_verts, comp ? 1 : 0);
+    lc.after("k_g3");
+}
+
+void launch_fast(const Level& Pl, const Level& L, int scheme, bool comp, Lc& lc)
+{
+    const bool lak = scheme == SLAK_SCHEME_LAK;
+    if (lak) {
+        if (L.make_state) launch_fast_t<true, true>(Pl, L, comp, lc);
+        else launch_fast_t<true, false>(Pl, L, comp, lc);
+    } else {
+        if (L.make_state) launch_fast_t<false, true>(Pl, L, comp, lc);
+        else launch_fast_t<false, false>(Pl, L, comp, lc);
+    }
+    if (L.o_ptr) {   // LAK final level: quad offsets and corner positions
+        k_quad_ptr_vals<<<grid_for(L.N), kBlock, 0, lc.s>>>((int)L.N, L.o_ptr, reinterpret_cast<int4*>(L.o_vals));
+        lc.after("k_quad_ptr_vals");
+    }
 }
 
 int enqueue_all(slak_plan* p, cudaStream_t str)
 {
     int64_t nl = 0;
+    Lc lc{str, &nl, p->debug, 0};
     cudaMemsetAsync(p->st, 0, sizeof(DevStatus), str);
     const bool comp = (p->flags & SLAK_PLAN_COMPENSATED) != 0;
     for (size_t li = 0; li < p->lv.size(); ++li) {
         const Level& L = p->lv[li];
-        launch_topology_a(L, (int)li, p->scheme, p->s, p->st, str, &nl);
+        lc.level = (int)li;
+        if (L.fast) {
+            launch_fast(p->lv[li - 1], L, p->scheme, comp, lc);
+            continue;
+        }
+        launch_topology_a(L, (int)li, p->scheme, p->s, p->st, lc);
         k_check_level<<<1, 1, 0, str>>>(p->s.eptr, (int)L.V, &p->st->bcount[li], (int)L.E, (int)L.B, p->st,
                                          (int)li);
-        ++nl;
-        if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, str, &nl);
-        else launch_rest<false>(L, p->scheme, comp, p->s, p->st, str, &nl);
+        lc.after("k_check_level");
+        if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, lc);
+        else launch_rest<false>(L, p->scheme, comp, p->s, p->st, lc);
+        if (L.export_state) {
+            k_export_state<<<grid_for(L.V), kBlock, 0, str>>>((int)L.V, p->s.sptr, p->s.sc, p->s.stw, p->s.xslot,
+                                                              p->s.xtw);
+            lc.after("k_export_state");
+            if (p->scheme == SLAK_SCHEME_SLAK) {
+                k_export_t<<<grid_for(L.N), kBlock, 0, str>>>((int)L.N, p->s.xslot, p->s.xtw, p->s.xt);
+                lc.after("k_export_t");
+            }
+        }
     }
     p->launches = nl;
-    return cuda_status(cudaGetLastError());
+    if (lc.err) return lc.err;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) g_detail = std::string("launch: ") + cudaGetErrorString(e);
+    return cuda_status(e);
 }
 
 void free_plan_memory(slak_plan* p)
@@ -243,14 +362,16 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str)
     carve_scratch(cv, s, L0.N, L0.V, 1, !L0.quad);
     DevStatus* st = cv.take<DevStatus>(1);
     int64_t nl = 0;
+    Lc lc{str, &nl, p->debug, 0};
     cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
-    launch_topology_a(L0, 0, p->scheme, s, st, str, &nl);
+    launch_topology_a(L0, 0, p->scheme, s, st, lc);
     cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
     cudaFree(mem);
-    if (e != cudaSuccess) return cuda_status(e);
-    if (p->h_st->err) return p->h_st->err;
+    if (lc.err) return lc.err;
+    if (e != cudaSuccess) { g_detail = std::string("level-0 probe: ") + cudaGetErrorString(e); return cuda_status(e); }
+    if (p->h_st->err) { g_detail = "level-0 probe: device detail " + std::to_string(p->h_st->detail); return p->h_st->err; }
     L0.B = p->h_st->bcount[0];
     L0.E = p->h_st->nedges;
     if (L0.E != (L0.N - L0.B) / 2 + L0.B) return SLAK_ERR_BAD_MESH;   // not a 2-manifold
@@ -278,6 +399,8 @@ const char* slak_status_string(int status)
 
 int slak_abi_version(void) { return SLAK_B200_ABI_VERSION; }
 
+const char* slak_last_error_detail(void) { return g_detail.c_str(); }
+
 int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flags, slak_stream_t stream,
                      slak_plan** out_plan)
 {
@@ -296,6 +419,10 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
     if (!p) return SLAK_ERR_OOM;
     p->scheme = scheme;
     p->flags = flags;
+    {
+        const char* dbg = std::getenv("SLAK_DEBUG_SYNC");
+        p->debug = dbg && dbg[0] == '1';
+    }
     p->in = *cm;
     cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
     int nlev = (quad_in ? 0 : 1);
@@ -314,6 +441,7 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
     L0.ptr = cm->ptr; L0.ids = cm->ids; L0.verts = cm->verts;
     int rc = probe_level0(p, L0, str);
     if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
+    const bool force_general = (flags & SLAK_PLAN_GENERAL) != 0;
     for (int i = 0; i < nlev; ++i) {
         Level& L = p->lv[i];
         if (i > 0) {
@@ -321,13 +449,27 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
             L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
             L.E = (L.N - L.B) / 2 + L.B;
             L.quad = true; L.poly_fn = false;
+            L.fast = !force_general && P.quad && P.B == 0;
         }
         L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
         if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) { free_plan_memory(p); delete p; return SLAK_ERR_UNSUPPORTED; }
-        if (L.N > p->maxN) p->maxN = L.N;
-        if (L.V > p->maxV) p->maxV = L.V;
-        if (L.E > p->maxE) p->maxE = L.E;
-        if (!L.quad) p->any_poly = true;
+        if (!L.fast) {
+            if (L.N > p->maxN) p->maxN = L.N;
+            if (L.V > p->maxV) p->maxV = L.V;
+            if (L.E > p->maxE) p->maxE = L.E;
+            if (!L.quad) p->any_poly = true;
+        }
+    }
+    int64_t exN = 0, stN = 0, stV = 0, stE = 0;
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) { L.export_state = true; if (L.N > exN) exN = L.N; }
+        if (L.fast && i + 1 < nlev && p->lv[i + 1].fast) {
+            L.make_state = true;
+            if (L.N > stN) stN = L.N;
+            if (L.V > stV) stV = L.V;
+            if (L.E > stE) stE = L.E;
+        }
     }
     // arena: scratch + ping-pong intermediates + status
     int64_t mid_ids = 0, mid_verts = 0;
@@ -337,6 +479,8 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
     }
     auto carve_all = [&](Carver& cv) {
         carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
+        if (exN) carve_export(cv, p->s, exN);
+        if (stN) { carve_state(cv, p->qs[0], stN, stV, stE); carve_state(cv, p->qs[1], stN, stV, stE); }
         for (int k = 0; k < 2; ++k) {
             p->ping_ids[k] = nlev > 1 ? cv.take<int>(mid_ids) : nullptr;
             p->ping_verts[k] = nlev > 1 ? cv.take<float>(4 * mid_verts) : nullptr;
@@ -377,6 +521,15 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
             L.o_ids = p->ping_ids[i & 1]; L.o_verts = p->ping_verts[i & 1];
         }
     }
+    int qi = 0;
+    for (int i = 1; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (!L.fast) continue;
+        const Level& P = p->lv[i - 1];
+        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.sc, p->s.xslot, p->s.xtw, p->s.xt, p->s.H};
+        else L.in_state = P.out_state;
+        if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
+    }
     *out_plan = p;
     return SLAK_OK;
 }
@@ -416,7 +569,8 @@ int slak_plan_status(slak_plan* p, slak_stream_t stream)
     cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemcpyAsync(p->h_st, p->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     if (e == cudaSuccess) e = cudaStreamSynchronize(str);
-    if (e != cudaSuccess) return cuda_status(e);
+    if (e != cudaSuccess) { g_detail = std::string("status: ") + cudaGetErrorString(e); return cuda_status(e); }
+    if (p->h_st->err) g_detail = "device detail " + std::to_string(p->h_st->detail);
     return p->h_st->err;
 }
 

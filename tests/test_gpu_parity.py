@@ -133,3 +133,23 @@ def test_bad_meshes_rejected():
     bad.ids[0:4] = bad.ids[4:8]               # duplicated face: non-manifold edges
     with pytest.raises(api._abi.SlakError):
         api.subdivide(bad, 1, SLAK)
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name,levels", [("torus32", 4), ("icosphere", 4), ("cylinder", 5), ("mixed", 4)])
+def test_fast_path_equals_general_path(name, levels, scheme):
+    """The closed-form levels (default) and the per-level general path give identical bits."""
+    m = meshgen.mixed_torus(64, 48, 0.05, 0.03, 0.005, seed=8) if name == "mixed" else meshgen.workload(name).mesh
+    fast = api.subdivide(m, levels, scheme)
+    gen = api.subdivide(m, levels, scheme, api._abi.PLAN_GENERAL)
+    assert np.array_equal(fast.ids, gen.ids)
+    assert _bits_equal(fast.verts, gen.verts)
+    if scheme == LAK:
+        assert np.array_equal(fast.ptr, gen.ptr) and np.array_equal(fast.vals, gen.vals)
+
+
+def test_fast_path_compensated_matches_general_compensated():
+    m = meshgen.workload("cylinder").mesh
+    a = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+    assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
