@@ -174,8 +174,8 @@ def run_ours(args, dist, rank, ws):
     value = faces * ws / (ms_step * 1e-3)
     launches = plan.launches * args.steps
 
-    # dominant kernel: per-kernel events from one instrumented eager execution
-    kern = plan_kernel_profile(plan, stream, torch)
+    # dominant kernel: per-kernel events of instrumented eager executions
+    kern, ktable = plan_kernel_profile(dm, levels, scheme, args.steps, stream, torch, flush)
 
     # e2e: host buffers, the C-ABI drop-in call
     e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws)
@@ -191,25 +191,57 @@ def run_ours(args, dist, rank, ws):
                    "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
                    "parallelism": f"replicas x{ws}"},
         "gpu_launches": launches,
-        "roofline": None,
+        "roofline": kern,
+        "kernels": ktable[:8],
         "pipeline_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                               "frac": achieved / peak, "peak_kind": peak_kind,
                               "algorithmic_bytes": alg_bytes},
         "e2e": e2e,
         "clocks": clk.summary(),
     }
-    if kern:
-        out["roofline"] = kern
     if rank == 0 and ws == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, levels, scheme, args.cpu_budget)
     plan.close()
     return out
 
 
-def plan_kernel_profile(plan, stream, torch):
-    """Per-level timing of one eager execution (a second plan without graph),
-    for the dominant-kernel roofline."""
-    return None
+def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush):
+    """Per-kernel device times from CUDA events recorded after every launch of an
+    eager execution (SLAK_PLAN_TIMING), averaged over `steps` timed executions
+    with the L2 flushed before each; returns the dominant kernel's roofline and
+    the per-kernel table."""
+    from slak_b200 import api
+    peak, peak_kind = _peaks()
+    with torch.cuda.stream(stream):
+        plan = api.Plan(dm, levels, scheme, api._abi.PLAN_TIMING, stream=stream)
+        plan.execute(stream)
+        plan.check(stream)
+        acc = {}
+        for i in range(steps):
+            flush.fill_(float(i))
+            plan.execute(stream)
+            for t in plan.kernel_timings():
+                key = (t["name"], t["level"])
+                a = acc.setdefault(key, [0.0, 0, t["algorithmic_bytes"]])
+                a[0] += t["ms"]
+                a[1] += 1
+        plan.check(stream)
+        plan.close()
+    table = []
+    for (name, level), (ms, cnt, b) in acc.items():
+        avg = ms / cnt
+        table.append({"kernel": name, "level": level, "ms": avg, "algorithmic_bytes": b,
+                      "GB/s": (b / (avg * 1e-3) / 1e9) if b and avg > 0 else None})
+    total = sum(t["ms"] for t in table)
+    for t in table:
+        t["share"] = t["ms"] / total if total else None
+    dom = max(table, key=lambda t: t["ms"])
+    achieved = dom["GB/s"] or 0.0
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "kernel": dom["kernel"], "level": dom["level"],
+            "kernel_ms": dom["ms"], "kernel_share": dom["share"], "peak_kind": f"{peak_kind} (copy bandwidth)",
+            "algorithmic_bytes_per_launch": dom["algorithmic_bytes"]}
+    return roof, sorted(table, key=lambda t: -t["ms"])
 
 
 def run_e2e(mesh, levels, scheme, args, torch, dist, ws):

@@ -108,8 +108,16 @@ typedef struct slak_plan slak_plan;
 enum slak_plan_flags {
     SLAK_PLAN_GRAPH = 1,        /* capture one execution as a CUDA graph and replay it       */
     SLAK_PLAN_GENERAL = 2,      /* run every level through the general per-level path         */
-    SLAK_PLAN_COMPENSATED = 4   /* compensated (TwoSum) sums in high-valence vertex points    */
+    SLAK_PLAN_COMPENSATED = 4,  /* compensated (TwoSum) sums in high-valence vertex points    */
+    SLAK_PLAN_TIMING = 8        /* record a CUDA event after every launch (per-kernel times)  */
 };
+
+typedef struct slak_kernel_timing {
+    const char* name;           /* kernel name (static string)                     */
+    int32_t level;              /* subdivision level it belongs to                 */
+    float ms;                   /* device time since the previous launch's event   */
+    int64_t algorithmic_bytes;  /* compulsory bytes it moves, 0 when not defined    */
+} slak_kernel_timing;
 
 typedef struct slak_level_stats {
     int64_t nfaces, nverts, nnz, nedges, nboundary;   /* of the level's input mesh */
@@ -128,6 +136,9 @@ int slak_plan_num_levels(const slak_plan* plan);
 int slak_plan_level_stats(const slak_plan* plan, int level, slak_level_stats* stats);
 /* Kernel launches one execution issues (the count a graph replays). */
 int64_t slak_plan_launches(const slak_plan* plan);
+/* Per-launch device times of the last execution of a SLAK_PLAN_TIMING plan
+ * (waits for it); returns the number of launches, or -status. */
+int slak_plan_kernel_timings(slak_plan* plan, slak_kernel_timing* out, int capacity);
 int slak_plan_destroy(slak_plan* plan);
 
 #ifdef __cplusplus

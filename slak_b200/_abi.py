@@ -14,12 +14,13 @@ SLAK_OK = 0
 STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: "SLAK_ERR_OOM",
                 4: "SLAK_ERR_BAD_MESH", 5: "SLAK_ERR_TIMEOUT", 6: "SLAK_ERR_UNSUPPORTED", 7: "SLAK_ERR_NOT_READY"}
 
-PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED = 1, 2, 4
+PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING = 1, 2, 4, 8
 
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free", "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
-           "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_destroy"]
+           "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
+           "slak_plan_destroy"]
 
 
 class SlakMesh(ctypes.Structure):
@@ -34,6 +35,11 @@ class LevelStats(ctypes.Structure):
     _fields_ = [("nfaces", ctypes.c_int64), ("nverts", ctypes.c_int64), ("nnz", ctypes.c_int64),
                 ("nedges", ctypes.c_int64), ("nboundary", ctypes.c_int64),
                 ("out_faces", ctypes.c_int64), ("out_verts", ctypes.c_int64),
+                ("algorithmic_bytes", ctypes.c_int64)]
+
+
+class KernelTiming(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("level", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("algorithmic_bytes", ctypes.c_int64)]
 
 
@@ -74,6 +80,8 @@ def lib():
         L.slak_plan_launches.argtypes = [V]
         L.slak_plan_launches.restype = I64
         L.slak_plan_destroy.argtypes = [V]
+        L.slak_plan_kernel_timings.argtypes = [V, ctypes.POINTER(KernelTiming), I]
+        L.slak_plan_kernel_timings.restype = I
         for n in ("slak_subdivide", "slak_mesh_free", "slak_plan_create", "slak_plan_execute", "slak_plan_status",
                   "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
                   "slak_plan_level_stats", "slak_plan_destroy"):

@@ -186,6 +186,15 @@ class Plan:
     def launches(self) -> int:
         return int(_abi.lib().slak_plan_launches(self._h))
 
+    def kernel_timings(self) -> List[dict]:
+        """Per-launch device times of the last execution (plan created with PLAN_TIMING)."""
+        buf = (_abi.KernelTiming * 512)()
+        n = _abi.lib().slak_plan_kernel_timings(self._h, buf, 512)
+        if n < 0:
+            _abi.check(-n, "slak_plan_kernel_timings")
+        return [{"name": buf[i].name.decode(), "level": int(buf[i].level), "ms": float(buf[i].ms),
+                 "algorithmic_bytes": int(buf[i].algorithmic_bytes)} for i in range(n)]
+
     def level_stats(self) -> List[dict]:
         out = []
         for i in range(_abi.lib().slak_plan_num_levels(self._h)):

@@ -77,7 +77,7 @@ def build_demo(verbose=False, force=False):
         return None
     hdrs = [os.path.join(_paths.INCLUDE_DIR, h) for h in ("CatmullClark.h", "LAKCatmullClark.h", "slak_b200.h")]
     if force or _stale(_paths.DEMO_BIN, src + hdrs + [_paths.LIB_SLAK, _paths.LIB_MESHGEN]):
-        cmd = [NVCC, "-std=c++17", "-O2", "-I", _paths.INCLUDE_DIR, "-o", _paths.DEMO_BIN] + src + [
+        cmd = [NVCC, "-std=c++17", "-O2", "-Wno-deprecated-gpu-targets", "-I", _paths.INCLUDE_DIR, "-o", _paths.DEMO_BIN] + src + [
             "-L", _paths.LIB_DIR, "-lslak_b200", "-lslak_meshgen", "-Xlinker", "-rpath=$ORIGIN"]
         _run(cmd, verbose)
     return _paths.DEMO_BIN

@@ -74,15 +74,27 @@ struct Carver {
 // and records which kernel failed.
 thread_local std::string g_detail;
 
+struct KernelRec {
+    const char* name;
+    int level;
+    int64_t bytes;
+};
+
 struct Lc {
     cudaStream_t s;
     int64_t* nl;
     bool debug;
     int level;
     int err = 0;
-    void after(const char* name, int n = 1)
+    std::vector<cudaEvent_t>* ev = nullptr;   // timing: one event after every launch (ev[0] before the first)
+    std::vector<KernelRec>* recs = nullptr;
+    void after(const char* name, int n = 1, int64_t bytes = 0)
     {
         *nl += n;
+        if (ev && recs->size() + 1 < ev->size()) {
+            cudaEventRecord((*ev)[recs->size() + 1], s);
+            recs->push_back(KernelRec{name, level, bytes});
+        }
         if (!debug || err) return;
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -125,6 +137,9 @@ struct slak_plan {
     int64_t launches = 0;
     int executed = 0;
     bool debug = false;
+    // per-launch timing (SLAK_PLAN_TIMING)
+    std::vector<cudaEvent_t> ev;
+    std::vector<KernelRec> recs;
 };
 
 namespace {
@@ -269,14 +284,19 @@ void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
 {
     FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N};
     cudaStream_t str = lc.s;
+    // compulsory bytes of each kernel: the level's corner ids and positions it
+    // must read once, and the refined ids / positions it alone writes
+    const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
+    const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
+    const int64_t g3b = 16 * Pl.V + (LAK ? 0 : 16 * L.F);
     k_g1<LAK, STATE><<<grid_for(L.N), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
                                                          reinterpret_cast<int4*>(L.o_ids), L.o_verts);
-    lc.after("k_g1");
+    lc.after("k_g1", 1, g1b);
     k_g2<LAK, STATE><<<grid_for(Pl.E), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
-    lc.after("k_g2");
+    lc.after("k_g2", 1, g2b);
     k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
                                                              L.o_verts, comp ? 1 : 0);
-    lc.after("k_g3");
+    lc.after("k_g3", 1, g3b);
 }
 
 void launch_fast(const Level& Pl, const Level& L, int scheme, bool comp, Lc& lc)
@@ -299,6 +319,16 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
 {
     int64_t nl = 0;
     Lc lc{str, &nl, p->debug, 0};
+    if (p->flags & SLAK_PLAN_TIMING) {
+        if (p->ev.empty()) {
+            p->ev.resize(512);
+            for (auto& e : p->ev) cudaEventCreate(&e);
+        }
+        p->recs.clear();
+        lc.ev = &p->ev;
+        lc.recs = &p->recs;
+        cudaEventRecord(p->ev[0], str);
+    }
     cudaMemsetAsync(p->st, 0, sizeof(DevStatus), str);
     const bool comp = (p->flags & SLAK_PLAN_COMPENSATED) != 0;
     for (size_t li = 0; li < p->lv.size(); ++li) {
@@ -333,6 +363,8 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
 
 void free_plan_memory(slak_plan* p)
 {
+    for (auto& e : p->ev) cudaEventDestroy(e);
+    p->ev.clear();
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     p->gexec = nullptr;
     if (p->arena) cudaFree(p->arena);
@@ -609,6 +641,23 @@ int slak_plan_level_stats(const slak_plan* p, int level, slak_level_stats* s)
 }
 
 int64_t slak_plan_launches(const slak_plan* p) { return p ? p->launches : 0; }
+
+int slak_plan_kernel_timings(slak_plan* p, slak_kernel_timing* out, int capacity)
+{
+    if (!p || (capacity > 0 && !out)) return -SLAK_ERR_INVALID_ARG;
+    if (!(p->flags & SLAK_PLAN_TIMING) || !p->executed) return -SLAK_ERR_NOT_READY;
+    if (cudaEventSynchronize(p->ev[p->recs.size()]) != cudaSuccess) return -SLAK_ERR_CUDA;
+    const int n = (int)p->recs.size();
+    for (int i = 0; i < n && i < capacity; ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]);
+        out[i].name = p->recs[i].name;
+        out[i].level = p->recs[i].level;
+        out[i].ms = ms;
+        out[i].algorithmic_bytes = p->recs[i].bytes;
+    }
+    return n;
+}
 
 int slak_plan_destroy(slak_plan* p)
 {
