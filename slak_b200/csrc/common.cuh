@@ -22,15 +22,27 @@ __device__ __forceinline__ float4 f4_mul(float4 a, float s)
 {
     return make_float4(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s), __fmul_rn(a.w, s));
 }
+// x / s.  When s is a normal power of two the quotient is an exact scaling, so
+// the product with the exact reciprocal 2^-e is the same correctly rounded
+// number (also under overflow / underflow) and avoids the IEEE divide sequence.
+__device__ __forceinline__ bool pow2_recip(float s, float& r)
+{
+    const unsigned u = __float_as_uint(s), ex = u & 0x7f800000u;
+    if ((u & 0x007fffffu) != 0u || ex == 0u || ex >= 0x7f000000u) return false;
+    r = __uint_as_float((0x7f000000u - ex) | (u & 0x80000000u));
+    return true;
+}
 __device__ __forceinline__ float4 f4_div(float4 a, float s)
 {
+    float r;
+    if (pow2_recip(s, r)) return f4_mul(a, r);
     return make_float4(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s), __fdiv_rn(a.w, s));
 }
 // x / s + 0.0f (turns -0 into +0, as an element-wise divide-then-add does)
 __device__ __forceinline__ float4 f4_div_z(float4 a, float s)
 {
-    return make_float4(__fadd_rn(__fdiv_rn(a.x, s), 0.0f), __fadd_rn(__fdiv_rn(a.y, s), 0.0f),
-                       __fadd_rn(__fdiv_rn(a.z, s), 0.0f), __fadd_rn(__fdiv_rn(a.w, s), 0.0f));
+    float4 q = f4_div(a, s);
+    return make_float4(__fadd_rn(q.x, 0.0f), __fadd_rn(q.y, 0.0f), __fadd_rn(q.z, 0.0f), __fadd_rn(q.w, 0.0f));
 }
 __device__ __forceinline__ float4 f4_zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 

@@ -23,11 +23,12 @@
 //         lower face point, higher face point}      [ascending (max, min)]
 //
 // Three kernels per level write every output exactly once, in contiguous runs:
-//   k_g1  per face of P (16 threads, one per corner of C): C's refined quads,
-//         face points of C, vertex points of the face points of P, SLAK edge
-//         points N1+x, and the next level's per-corner state
+//   k_g1  per quad of C (4 threads per face of P): C's refined quads, face
+//         points of C, vertex points of the face points of P, SLAK edge points
+//         N1+x, and the next level's per-corner state
 //   k_g2  per edge of P: vertex points of the edge points of P, LAK edge points
-//   k_g3  per vertex of P: vertex points of P's vertices, SLAK edge points slot1(x)
+//   k_g3v per vertex of P: vertex points of P's vertices
+//   k_g3e per slot of P: SLAK edge points slot1(x), C's old columns
 // The float arithmetic and its order are exactly the general path's (and the
 // reference's serialized order), so both paths are bit-identical.
 #pragma once
@@ -69,117 +70,124 @@ __device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
 __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a) + (c < a) + (d < a); }
 
 // ---------------------------------------------------------------------------------------------
-// G1: one thread per corner y of C; the 16 corners of a face g of P are 16 consecutive lanes.
+// G1: one thread per quad x of C (= corner x of P); the 4 quads of a face of P
+// are 4 consecutive lanes.  Each thread loads its quad {v, e_out, f, e_in} as
+// one int4 and the 4 corner positions, so the face point needs no exchange;
+// the block stages its 4 x 256 refined quads in shared memory and stores them
+// as one contiguous 16 KB run.
 template <bool LAK, bool STATE>
 __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
                                                QState p, QState c, int4* __restrict__ out_ids,
                                                float* __restrict__ R)
 {
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = y < d.N;
-    const int lane = threadIdx.x & 31;
-    const int qb = lane & ~3;            // lane of corner 0 of my quad
-    const int gb = lane & ~15;           // lane of corner 0 of my group's quad 0
-    const int x = y >> 2, k = y & 3, q = x & 3;
+    __shared__ int4 sq[4 * kBlock];
+    const int x0 = blockIdx.x * blockDim.x;
+    const int x = x0 + threadIdx.x;
+    const bool valid = x < d.N1;
+    const int lane = threadIdx.x & 31, q = x & 3;
+    const int gl = lane & ~3;                  // lane of quad 0 of my face of P
     const int VF1 = d.V1 + d.F1;
-    const int VFc = d.V + d.N1;          // C: V + F
+    const int VFc = d.V + d.N1;                // C: V + F
 
-    const int vid = valid ? __ldg(ids + y) : 0;
-    const float4 pos = valid ? ldg4(P, vid) : f4_zero();
+    const int4 Q = valid ? __ldg(reinterpret_cast<const int4*>(ids) + x) : make_int4(0, 0, 0, 0);
+    const float4 c0 = valid ? ldg4(P, Q.x) : f4_zero();
+    const float4 c1 = valid ? ldg4(P, Q.y) : f4_zero();
+    const float4 c2 = valid ? ldg4(P, Q.z) : f4_zero();
+    const float4 c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
     if (valid && (LAK || STATE)) tw1x = __ldg(p.tw + x);
     if (valid && !LAK) { s1 = __ldg(p.slot + x); t1x = __ldg(p.t + x); }
-
-    // values from the other corners / quads of the group
-    const int lq_next = gb | (((q + 1) & 3) << 2), lq_prev = gb | (((q + 3) & 3) << 2);
-    const int v1 = __shfl_sync(0xffffffffu, vid, qb + 1);              // e_out(x) id
-    const int v3 = __shfl_sync(0xffffffffu, vid, qb + 3);              // e_in(x) id
-    const int tw1_px = __shfl_sync(0xffffffffu, tw1x, lq_prev);        // tw1(prev x)
-    const int eidp_x = v1 - VF1, eidp_px = v3 - VF1;                   // P's edge ids of x, prev(x)
-
-    int eid;
-    if (!LAK) {
-        eid = k == 0 ? s1 : k == 1 ? d.N1 + qnext(x) : k == 2 ? d.N1 + x : t1x;
-    } else {
-        const int vx = __shfl_sync(0xffffffffu, vid, qb);
-        const int vnx = __shfl_sync(0xffffffffu, vid, lq_next);
-        const int vpx = __shfl_sync(0xffffffffu, vid, lq_prev);
-        const int fx = x >> 2;
-        eid = k == 0 ? 4 * eidp_x + (vx > vnx)
-            : k == 1 ? 4 * eidp_x + 2 + (fx > (tw1x >> 2))
-            : k == 2 ? 4 * eidp_px + 2 + (fx > (tw1_px >> 2))
-                     : 4 * eidp_px + (vx > vpx);
-    }
-    const int ein = __shfl_sync(0xffffffffu, eid, qb + ((k + 3) & 3));
-    if (valid) __stcs(out_ids + y, make_int4(vid, VFc + eid, d.V + x, VFc + ein));
+    const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
+    const int tw1_px = __shfl_sync(0xffffffffu, tw1x, lp);
+    const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
 
     // face point of quad x
     float4 fp;
     if (!LAK) {
-        float4 a = f4_add(pos, shfl4_xor(pos, 2));
-        fp = f4_mul(f4_add(a, shfl4_xor(a, 1)), 0.25f);
+        fp = f4_mul(f4_add(f4_add(c0, c2), f4_add(c1, c3)), 0.25f);
     } else {
-        float4 acc = f4_add(f4_zero(), shfl4(pos, qb));
-        acc = f4_add(acc, shfl4(pos, qb + 1));
-        acc = f4_add(acc, shfl4(pos, qb + 2));
-        acc = f4_add(acc, shfl4(pos, qb + 3));
-        fp = f4_div_z(acc, 4.0f);
+        fp = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), c1), c2), c3), 4.0f);
     }
-    if (valid && k == 0) st4(R, (int64_t)d.V + x, fp);
 
-    // vertex point of the face point V1 + g (corners 4x+2 of the group's quads, n = 4)
+    // edge ids of C's corners 4x+k
+    int e0, e1, e2, e3;
+    if (!LAK) {
+        e0 = s1; e1 = d.N1 + qnext(x); e2 = d.N1 + x; e3 = t1x;
+    } else {
+        const int vnx = __shfl_sync(0xffffffffu, Q.x, ln), vpx = __shfl_sync(0xffffffffu, Q.x, lp);
+        const int fx = x >> 2;
+        e0 = 4 * eidp_x + (Q.x > vnx);
+        e1 = 4 * eidp_x + 2 + (fx > (tw1x >> 2));
+        e2 = 4 * eidp_px + 2 + (fx > (tw1_px >> 2));
+        e3 = 4 * eidp_px + (Q.x > vpx);
+    }
+    // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}: staged, then one coalesced run
+    const int fpid = d.V + x;
+    sq[4 * threadIdx.x + 0] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
+    sq[4 * threadIdx.x + 1] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
+    sq[4 * threadIdx.x + 2] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
+    sq[4 * threadIdx.x + 3] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
+    __syncthreads();
     {
-        float4 nb[4], fq[4];
+        const int nq = min(kBlock, d.N1 - x0);
+        int4* dst = out_ids + 4 * (int64_t)x0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            nb[j] = shfl4(pos, gb | (j << 2) | (LAK ? 1 : 3));   // SLAK: e_in(x) positions; LAK: tails e_out(x)
-            fq[j] = shfl4(fp, gb | (j << 2));
+        for (int i = 0; i < 4; ++i) {
+            const int j = i * kBlock + threadIdx.x;
+            if (j < 4 * nq) __stcs(dst + j, sq[j]);
         }
-        const float4 pf = shfl4(pos, gb | 2);
+    }
+    if (valid) st4(R, (int64_t)d.V + x, fp);
+
+    // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
+    float4 nb[4], fq[4];
+    int tl[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        nb[j] = shfl4(LAK ? c1 : c3, gl | j);      // SLAK: e_in(x_j); LAK: tails e_out(x_j)
+        fq[j] = shfl4(fp, gl | j);
+        tl[j] = __shfl_sync(0xffffffffu, Q.y, gl | j);
+    }
+    if (valid && q == 0) {
         float4 yv;
         if (!LAK) {
             float4 acc = f4_zero();
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc = f4_add(acc, nb[j]);
-            yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(pf, 2.0f), 4.0f));
+            yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(c2, 2.0f), 4.0f));
 #pragma unroll
             for (int j = 0; j < 4; ++j) yv = f4_add(yv, f4_div(fq[j], 16.0f));
         } else {
-            int tid[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) tid[j] = __shfl_sync(0xffffffffu, vid, gb | (j << 2) | 1);
             float4 acc = f4_zero();
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc = f4_add(acc, fq[j]);
-            // tails in ascending vertex id
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     int rk = 0;
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) rk += tid[i] < tid[j];
+                    for (int i = 0; i < 4; ++i) rk += tl[i] < tl[j];
                     if (rk == r) acc = f4_add(acc, nb[j]);
                 }
             }
-            yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(pf, 2.0f)), 4.0f);
+            yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(c2, 2.0f)), 4.0f);
         }
-        if (valid && (lane & 15) == 0) st4(R, (int64_t)d.V1 + (x >> 2), yv);
+        st4(R, (int64_t)d.V1 + (x >> 2), yv);
     }
 
     // SLAK edge point N1 + x: half-edges 4x+2 (tail f, quad x) and 4 prev(x)+1 (tail e_in(x), quad prev x)
     if (!LAK) {
-        const float4 fprev = shfl4(fp, lq_prev);
-        const float4 pf = shfl4(pos, qb + 2), pin = shfl4(pos, qb + 3);
-        if (valid && k == 2) {
-            float4 ta = f4_mul(f4_add(pf, fp), 0.25f);
-            float4 tb = f4_mul(f4_add(pin, fprev), 0.25f);
+        const float4 fprev = shfl4(fp, lp);
+        if (valid) {
+            float4 ta = f4_mul(f4_add(c2, fp), 0.25f);
+            float4 tb = f4_mul(f4_add(c3, fprev), 0.25f);
             st4_cs(R, (int64_t)VFc + d.N1 + x, f4_add(f4_add(f4_zero(), ta), tb));
         }
     }
 
     if (STATE && valid) {
-        // C's slot / twin / t for corner y
+        // C's slot / twin / t for corners 4x+k
         const int px = qprev(x), nxx = qnext(x);
         const int ntw = qnext(tw1x), ntwp = qnext(tw1_px);
         // edge of P through x: corners A=4x+1, B=4tw1x+1, Cc=4nxx+3, D=4ntw+3
@@ -187,25 +195,16 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
         // edge of P through prev(x): A'=4px+1, B'=4tw1_px+1, C'=4x+3, D'=4ntwp+3
         const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
         const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
-        int sl, tw;
-        if (k == 0) { sl = s1; tw = 4 * ntw + 3; }
-        else if (k == 1) { sl = base_x + rank4(A, B, Cc, D); tw = 4 * nxx + 2; }
-        else if (k == 2) { sl = d.N1 + x; tw = 4 * px + 1; }
-        else { sl = base_px + rank4(C2, A2, B2, D2); tw = 4 * tw1_px; }
-        c.slot[y] = sl;
-        c.tw[y] = tw;
+        reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
         if (!LAK) {
-            int tt = k == 0 ? t1x
-                   : k == 1 ? base_x + rank4(D, A, B, Cc)
-                   : k == 2 ? d.N1 + nxx
-                            : base_px + rank4(A2, B2, C2, D2);
-            c.t[y] = tt;
+            reinterpret_cast<int4*>(c.slot)[x] =
+                make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
+            reinterpret_cast<int4*>(c.t)[x] =
+                make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
+            c.H[d.N1 + x] = make_int2(4 * x + 2, 4 * px + 1);     // SLAK edge N1 + x
         }
-        if (k == 2) {
-            c.sc[d.N1 + x] = y;                                   // face point column
-            if (!LAK) c.H[d.N1 + x] = make_int2(y, 4 * px + 1);   // SLAK edge N1 + x
-        }
-        if ((lane & 15) == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + 4 * (x >> 2);
+        c.sc[d.N1 + x] = 4 * x + 2;                                // face point column
+        if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
     }
 }
 
@@ -287,10 +286,12 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict
 }
 
 // ---------------------------------------------------------------------------------------------
-// G3: one thread per vertex v of P (its column of corners x, each giving C's corner 4x)
+// G3v: one thread per vertex v of P: its vertex point (corners 4x of C, x in v's column).
+// The first 4 column entries are loaded up front (valence 4 dominates refined
+// meshes); longer columns continue in a loop, in the same order.
 template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
-                                               QState p, QState c, float* __restrict__ R, int compensated)
+__global__ void __launch_bounds__(kBlock) k_g3v(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
+                                                QState p, QState c, float* __restrict__ R, int compensated)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= d.V1) {
@@ -299,59 +300,97 @@ __global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const int* __restrict
     }
     const int b = __ldg(p.sptr + v), e = __ldg(p.sptr + v + 1), n = e - b;
     const float* FP = R + 4 * (int64_t)d.V;
+    constexpr int U = 4;
+    int xs[U], tv[U];
+    float4 fx[U], pv[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) xs[j] = j < n ? __ldg(p.sc + b + j) : 0;
+#pragma unroll
+    for (int j = 0; j < U; ++j) tv[j] = j < n ? __ldg(ids + 4 * xs[j] + (LAK ? 3 : 1)) : 0;  // e_in / e_out of x
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+        fx[j] = j < n ? ldg4(FP, xs[j]) : f4_zero();
+        pv[j] = j < n ? ldg4(P, tv[j]) : f4_zero();
+    }
     const float4 Pv = ldg4(P, v);
     const float nn = (float)(n * n);
-    const int64_t EPb = (int64_t)d.V + d.N1;       // C's edge points start at V + F
     float4 yv;
+    const bool comp = compensated && n > 4;
     if (!LAK) {
-        if (!compensated || n <= 4) {
+        if (!comp) {
             float4 acc = f4_zero();
-            for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
+#pragma unroll
+            for (int j = 0; j < U; ++j) if (j < n) acc = f4_add(acc, pv[j]);
+            for (int s = b + U; s < e; ++s) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
             yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
-            for (int s = b; s < e; ++s) yv = f4_add(yv, f4_div(ldg4(FP, __ldg(p.sc + s)), nn));
+#pragma unroll
+            for (int j = 0; j < U; ++j) if (j < n) yv = f4_add(yv, f4_div(fx[j], nn));
+            for (int s = b + U; s < e; ++s) yv = f4_add(yv, f4_div(ldg4(FP, __ldg(p.sc + s)), nn));
         } else {
             float4 sh = f4_zero(), sl = f4_zero();
             for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
             for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, __ldg(p.sc + s)));
             yv = vp_finish(sh, sl, Pv, n);
         }
-        // edge points of C's edges {v, e_out(x)}: ids slot1(x) = s
-        for (int s = b; s < e; ++s) {
-            const int x = __ldg(p.sc + s);
-            const int tw = __ldg(p.tw + x);
-            const int eo = __ldg(ids + 4 * x + 1);
-            float4 ta = f4_mul(f4_add(Pv, ldg4(FP, x)), 0.25f);
-            float4 tb = f4_mul(f4_add(ldg4(P, eo), ldg4(FP, qnext(tw))), 0.25f);
-            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), tb));
-            if (STATE) c.H[s] = make_int2(4 * x, 4 * qnext(tw) + 3);
-        }
     } else {
         // face points in column order, then the tails e_in(x) in ascending id
         float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
-        const bool comp = compensated && n > 4;
-        for (int s = b; s < e; ++s) {
+#pragma unroll
+        for (int j = 0; j < U; ++j) if (j < n) { if (comp) dd_acc(sh, sl, fx[j]); else acc = f4_add(acc, fx[j]); }
+        for (int s = b + U; s < e; ++s) {
             float4 f = ldg4(FP, __ldg(p.sc + s));
             if (comp) dd_acc(sh, sl, f); else acc = f4_add(acc, f);
         }
-        int last = -1;
-        while (true) {
-            int xm = INT32_MAX;
-            for (int s = b; s < e; ++s) {
-                int ti = __ldg(ids + 4 * __ldg(p.sc + s) + 3);
-                if (ti > last && ti < xm) xm = ti;
+        if (n <= U) {
+#pragma unroll
+            for (int r = 0; r < U; ++r) {
+#pragma unroll
+                for (int j = 0; j < U; ++j) {
+                    int rk = 0;
+#pragma unroll
+                    for (int i = 0; i < U; ++i) rk += (i < n) && tv[i] < tv[j];
+                    if (j < n && rk == r) { if (comp) dd_acc(sh, sl, pv[j]); else acc = f4_add(acc, pv[j]); }
+                }
             }
-            if (xm == INT32_MAX) break;
-            if (comp) dd_acc(sh, sl, ldg4(P, xm)); else acc = f4_add(acc, ldg4(P, xm));
-            last = xm;
+        } else {
+            int last = -1;
+            while (true) {
+                int xm = INT32_MAX;
+                for (int s = b; s < e; ++s) {
+                    int ti = __ldg(ids + 4 * __ldg(p.sc + s) + 3);
+                    if (ti > last && ti < xm) xm = ti;
+                }
+                if (xm == INT32_MAX) break;
+                if (comp) dd_acc(sh, sl, ldg4(P, xm)); else acc = f4_add(acc, ldg4(P, xm));
+                last = xm;
+            }
         }
         if (comp) yv = vp_finish(sh, sl, Pv, n);
         else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
     }
     st4(R, v, yv);
-    if (STATE) {
-        c.sptr[v] = b;
-        for (int s = b; s < e; ++s) c.sc[s] = 4 * __ldg(p.sc + s);
-    }
+    if (STATE) c.sptr[v] = b;
+}
+
+// G3e: one thread per slot s of P (corner x = sc1[s] of vertex v): C's edge
+// {v, e_out(x)} has id s in SLAK order; its edge point and state are written
+// at s (coalesced).  LAK only copies the column entry.
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_g3e(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
+                                                QState p, QState c, float* __restrict__ R)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.N1) return;
+    const int x = __ldg(p.sc + s);
+    if (STATE) c.sc[s] = 4 * x;
+    if (LAK) return;
+    const int2 ve = __ldg(reinterpret_cast<const int2*>(ids) + 2 * x);      // {v, e_out(x)} of quad x
+    const int tw = __ldg(p.tw + x);
+    const float* FP = R + 4 * (int64_t)d.V;
+    float4 ta = f4_mul(f4_add(ldg4(P, ve.x), ldg4(FP, x)), 0.25f);
+    float4 tb = f4_mul(f4_add(ldg4(P, ve.y), ldg4(FP, qnext(tw))), 0.25f);
+    st4_cs(R, (int64_t)d.V + d.N1 + s, f4_add(f4_add(f4_zero(), ta), tb));
+    if (STATE) c.H[s] = make_int2(4 * x, 4 * qnext(tw) + 3);
 }
 
 // ---------------------------------------------------------------------------------------------

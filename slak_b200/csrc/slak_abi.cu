@@ -288,15 +288,18 @@ void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
     // must read once, and the refined ids / positions it alone writes
     const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
-    const int64_t g3b = 16 * Pl.V + (LAK ? 0 : 16 * L.F);
-    k_g1<LAK, STATE><<<grid_for(L.N), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
+    k_g1<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
                                                          reinterpret_cast<int4*>(L.o_ids), L.o_verts);
     lc.after("k_g1", 1, g1b);
     k_g2<LAK, STATE><<<grid_for(Pl.E), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
     lc.after("k_g2", 1, g2b);
-    k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
-                                                             L.o_verts, comp ? 1 : 0);
-    lc.after("k_g3", 1, g3b);
+    k_g3v<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
+                                                              L.o_verts, comp ? 1 : 0);
+    lc.after("k_g3v", 1, 16 * Pl.V);
+    if (!LAK || STATE) {
+        k_g3e<LAK, STATE><<<grid_for(Pl.N), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+        lc.after("k_g3e", 1, LAK ? 0 : 16 * L.F);
+    }
 }
 
 void launch_fast(const Level& Pl, const Level& L, int scheme, bool comp, Lc& lc)
