@@ -141,6 +141,29 @@ int64_t slak_plan_launches(const slak_plan* plan);
 int slak_plan_kernel_timings(slak_plan* plan, slak_kernel_timing* out, int capacity);
 int slak_plan_destroy(slak_plan* plan);
 
+/*
+ * Batches: many meshes, each with its own target level, refined by one call
+ * (what the reference's config-file loop does one mesh at a time,
+ * source/main.cpp:84-113).  Each mesh's result is exactly slak_subdivide's on
+ * that mesh alone.  All sizes are fixed at creation (one stream sync for all
+ * meshes' level-0 topology); every output lives in one batch-owned buffer
+ * (slak_batch_output returns views, valid until slak_batch_destroy); plans
+ * share device scratch in waves sized to the free memory; within a wave,
+ * meshes run concurrently on parallel streams.  With SLAK_PLAN_GRAPH the whole
+ * batch is captured as one CUDA graph on the first execution.
+ */
+typedef struct slak_batch slak_batch;
+int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
+                      slak_stream_t stream, slak_batch** batch);
+int slak_batch_execute(slak_batch* batch, slak_stream_t stream);
+/* Waits for `stream`, then reports the first failing mesh's device status. */
+int slak_batch_status(slak_batch* batch, slak_stream_t stream);
+/* The refined mesh of meshes[index]; left untouched when that mesh had nothing to refine. */
+int slak_batch_output(const slak_batch* batch, int64_t index, slak_mesh* rmesh);
+int slak_batch_num_waves(const slak_batch* batch);
+int64_t slak_batch_launches(const slak_batch* batch);
+int slak_batch_destroy(slak_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

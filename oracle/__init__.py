@@ -81,7 +81,8 @@ def _as_or(mesh, keep):
     m.ids = p(mesh.ids.astype(np.int32), ctypes.c_int32)
     m.vals = p(None if mesh.vals is None else mesh.vals.astype(np.int32), ctypes.c_int32)
     m.verts = p(mesh.verts.astype(np.float32).reshape(-1), ctypes.c_float)
-    m.verts64 = None
+    v64 = getattr(mesh, "verts64", None)
+    m.verts64 = p(None if v64 is None else np.asarray(v64, np.float64).reshape(-1), ctypes.c_double)
     return m
 
 
@@ -109,3 +110,32 @@ def level(mesh, scheme: int, poly: bool, fp64: bool = False) -> Result:
     res = Result(out)
     lib().or_mesh_free(ctypes.byref(out))
     return res
+
+
+class _LevelMesh:
+    """Adapter: an oracle Result as the input of the next oracle level."""
+
+    def __init__(self, r: Result):
+        self.type, self.is_reduced = r.type, r.is_reduced
+        self.nfaces, self.nverts, self.nnz = r.nfaces, r.nverts, r.nnz
+        self.max_face_order = r.max_face_order or 4
+        self.ptr, self.ids, self.vals = r.ptr, r.ids, r.vals
+        self.verts, self.verts64 = r.verts, r.verts64
+
+
+def subdivide_levels(mesh, levels: int, scheme: int):
+    """Every level's oracle result (FP32 and FP64 positions), level 1 first.
+    The FP64 shadow of level l feeds level l+1, so level l's verts64 is the
+    FP64 evaluation of l levels of the same subdivision matrices."""
+    out = []
+    cur = mesh
+    if getattr(cur, "verts64", None) is None:
+        cur = _LevelMesh.__new__(_LevelMesh)
+        for f in ("type", "is_reduced", "nfaces", "nverts", "nnz", "max_face_order", "ptr", "ids", "vals", "verts"):
+            setattr(cur, f, getattr(mesh, f))
+        cur.verts64 = mesh.verts.astype(np.float64)
+    for l in range(levels):
+        r = level(cur, scheme, poly=(l == 0 and mesh.type != 1), fp64=True)
+        out.append(r)
+        cur = _LevelMesh(r)
+    return out

@@ -17,10 +17,12 @@ STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: 
 PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING = 1, 2, 4, 8
 
 # every symbol include/slak_b200.h declares
-EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free", "slak_plan_create",
+EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
+           "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
-           "slak_plan_destroy"]
+           "slak_plan_destroy", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
+           "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
 
 
 class SlakMesh(ctypes.Structure):
@@ -82,6 +84,17 @@ def lib():
         L.slak_plan_destroy.argtypes = [V]
         L.slak_plan_kernel_timings.argtypes = [V, ctypes.POINTER(KernelTiming), I]
         L.slak_plan_kernel_timings.restype = I
+        L.slak_batch_create.argtypes = [P, ctypes.POINTER(ctypes.c_int), I64, I, I, V, ctypes.POINTER(V)]
+        L.slak_batch_execute.argtypes = [V, V]
+        L.slak_batch_status.argtypes = [V, V]
+        L.slak_batch_output.argtypes = [V, I64, P]
+        L.slak_batch_num_waves.argtypes = [V]
+        L.slak_batch_launches.argtypes = [V]
+        L.slak_batch_launches.restype = I64
+        L.slak_batch_destroy.argtypes = [V]
+        for n in ("slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
+                  "slak_batch_num_waves", "slak_batch_destroy"):
+            getattr(L, n).restype = I
         for n in ("slak_subdivide", "slak_mesh_free", "slak_plan_create", "slak_plan_execute", "slak_plan_status",
                   "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
                   "slak_plan_level_stats", "slak_plan_destroy"):

@@ -223,3 +223,51 @@ def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0) -> Ho
     torch.cuda.synchronize()
     plan.close()
     return out
+
+
+class Batch:
+    """Many meshes, each with its own level count, in one call (slak_batch_*).
+
+    ``meshes`` are DeviceMesh inputs; outputs are views into the batch's
+    memory, valid while the Batch lives."""
+
+    def __init__(self, meshes: List[DeviceMesh], levels: List[int], scheme: int, flags: int = 0, stream=None):
+        self._meshes = list(meshes)
+        n = len(self._meshes)
+        self._arr = (_abi.SlakMesh * max(n, 1))()
+        for i, m in enumerate(self._meshes):
+            self._arr[i] = m.as_c()
+        self._levels = (ctypes.c_int * max(n, 1))(*[int(l) for l in levels])
+        h = ctypes.c_void_p()
+        rc = _abi.lib().slak_batch_create(self._arr, self._levels, n, int(scheme), int(flags),
+                                          _stream_handle(stream), ctypes.byref(h))
+        _abi.check(rc, "slak_batch_create")
+        self._h = h
+        self.count = n
+
+    def execute(self, stream=None) -> None:
+        _abi.check(_abi.lib().slak_batch_execute(self._h, _stream_handle(stream)), "slak_batch_execute")
+
+    def check(self, stream=None) -> None:
+        _abi.check(_abi.lib().slak_batch_status(self._h, _stream_handle(stream)), "slak_batch_status")
+
+    def output(self, i: int) -> Optional[DeviceMesh]:
+        c = _abi.SlakMesh()
+        _abi.check(_abi.lib().slak_batch_output(self._h, int(i), ctypes.byref(c)), "slak_batch_output")
+        return _wrap_c(c, self) if c.ids else None
+
+    @property
+    def waves(self) -> int:
+        return int(_abi.lib().slak_batch_num_waves(self._h))
+
+    @property
+    def launches(self) -> int:
+        return int(_abi.lib().slak_batch_launches(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _abi.lib().slak_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -27,8 +27,8 @@
 //         points of C, vertex points of the face points of P, SLAK edge points
 //         N1+x, and the next level's per-corner state
 //   k_g2  per edge of P: vertex points of the edge points of P, LAK edge points
-//   k_g3v per vertex of P: vertex points of P's vertices
-//   k_g3e per slot of P: SLAK edge points slot1(x), C's old columns
+//   k_g3  per vertex of P: vertex points of P's vertices and SLAK edge points
+//         slot1(x), streamed from slot-ordered records k_g1 scatters
 // The float arithmetic and its order are exactly the general path's (and the
 // reference's serialized order), so both paths are bit-identical.
 #pragma once
@@ -75,10 +75,21 @@ __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a
 // one int4 and the 4 corner positions, so the face point needs no exchange;
 // the block stages its 4 x 256 refined quads in shared memory and stores them
 // as one contiguous 16 KB run.
+// Slot-ordered records for the per-vertex pass (k_g3): for the corner x of P
+// at slot s = slot1(x), Z[2s] = FP(x) and Z[2s+1] = the position of C's next
+// (SLAK: e_out(x)) or previous (LAK: e_in(x)) vertex of corner 4x; T[s] = that
+// vertex id (LAK ordering); B[t1(x)] = (P[e_in(x)] + FP(x)) / 4, the half of the
+// SLAK edge point t1(x) contributed by half-edge 4x+3.
+struct SlotScratch {
+    float4* Z;
+    float4* B;
+    int* T;
+};
+
 template <bool LAK, bool STATE>
 __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
                                                QState p, QState c, int4* __restrict__ out_ids,
-                                               float* __restrict__ R)
+                                               float* __restrict__ R, SlotScratch z)
 {
     __shared__ int4 sq[4 * kBlock];
     const int x0 = blockIdx.x * blockDim.x;
@@ -96,7 +107,8 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
     const float4 c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
     if (valid && (LAK || STATE)) tw1x = __ldg(p.tw + x);
-    if (valid && !LAK) { s1 = __ldg(p.slot + x); t1x = __ldg(p.t + x); }
+    if (valid) s1 = __ldg(p.slot + x);
+    if (valid && !LAK) t1x = __ldg(p.t + x);
     const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
     const int tw1_px = __shfl_sync(0xffffffffu, tw1x, lp);
     const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
@@ -137,7 +149,14 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
             if (j < 4 * nq) __stcs(dst + j, sq[j]);
         }
     }
-    if (valid) st4(R, (int64_t)d.V + x, fp);
+    if (valid) {
+        st4(R, (int64_t)d.V + x, fp);
+        // records of corner x for its vertex's pass (full 32-byte sectors at slot s1)
+        z.Z[2 * (int64_t)s1] = fp;
+        z.Z[2 * (int64_t)s1 + 1] = LAK ? c3 : c1;
+        if (LAK) z.T[s1] = Q.w;
+        else z.B[t1x] = f4_mul(f4_add(c3, fp), 0.25f);
+    }
 
     // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
     float4 nb[4], fq[4];
@@ -196,9 +215,11 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
         const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
         const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
         reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
+        reinterpret_cast<int4*>(c.slot)[x] =
+            make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
+        c.sc[s1] = 4 * x;                                          // old vertex column, slot s1
         if (!LAK) {
-            reinterpret_cast<int4*>(c.slot)[x] =
-                make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
+            c.H[s1] = make_int2(4 * x, 4 * ntw + 3);               // SLAK edge slot1(x)
             reinterpret_cast<int4*>(c.t)[x] =
                 make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
             c.H[d.N1 + x] = make_int2(4 * x + 2, 4 * px + 1);     // SLAK edge N1 + x
@@ -286,12 +307,12 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict
 }
 
 // ---------------------------------------------------------------------------------------------
-// G3v: one thread per vertex v of P: its vertex point (corners 4x of C, x in v's column).
-// The first 4 column entries are loaded up front (valence 4 dominates refined
-// meshes); longer columns continue in a loop, in the same order.
+// G3: one thread per vertex v of P.  Its column's records (written by k_g1 at
+// the column's slots) are contiguous, so the vertex point and, for SLAK, the
+// edge points of C's edges {v, e_out(x)} (ids = the slots) stream.
 template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g3v(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
-                                                QState p, QState c, float* __restrict__ R, int compensated)
+__global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
+                                               SlotScratch z, float* __restrict__ R, int compensated)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= d.V1) {
@@ -299,98 +320,53 @@ __global__ void __launch_bounds__(kBlock) k_g3v(FastDims d, const int* __restric
         return;
     }
     const int b = __ldg(p.sptr + v), e = __ldg(p.sptr + v + 1), n = e - b;
-    const float* FP = R + 4 * (int64_t)d.V;
-    constexpr int U = 4;
-    int xs[U], tv[U];
-    float4 fx[U], pv[U];
-#pragma unroll
-    for (int j = 0; j < U; ++j) xs[j] = j < n ? __ldg(p.sc + b + j) : 0;
-#pragma unroll
-    for (int j = 0; j < U; ++j) tv[j] = j < n ? __ldg(ids + 4 * xs[j] + (LAK ? 3 : 1)) : 0;  // e_in / e_out of x
-#pragma unroll
-    for (int j = 0; j < U; ++j) {
-        fx[j] = j < n ? ldg4(FP, xs[j]) : f4_zero();
-        pv[j] = j < n ? ldg4(P, tv[j]) : f4_zero();
-    }
     const float4 Pv = ldg4(P, v);
     const float nn = (float)(n * n);
+    const float4* Z = z.Z;
     float4 yv;
     const bool comp = compensated && n > 4;
     if (!LAK) {
         if (!comp) {
             float4 acc = f4_zero();
-#pragma unroll
-            for (int j = 0; j < U; ++j) if (j < n) acc = f4_add(acc, pv[j]);
-            for (int s = b + U; s < e; ++s) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
+            for (int s = b; s < e; ++s) acc = f4_add(acc, __ldg(Z + 2 * (int64_t)s + 1));
             yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
-#pragma unroll
-            for (int j = 0; j < U; ++j) if (j < n) yv = f4_add(yv, f4_div(fx[j], nn));
-            for (int s = b + U; s < e; ++s) yv = f4_add(yv, f4_div(ldg4(FP, __ldg(p.sc + s)), nn));
+            for (int s = b; s < e; ++s) yv = f4_add(yv, f4_div(__ldg(Z + 2 * (int64_t)s), nn));
         } else {
             float4 sh = f4_zero(), sl = f4_zero();
-            for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(P, __ldg(ids + 4 * __ldg(p.sc + s) + 1)));
-            for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, __ldg(p.sc + s)));
+            for (int s = b; s < e; ++s) dd_acc(sh, sl, __ldg(Z + 2 * (int64_t)s + 1));
+            for (int s = b; s < e; ++s) dd_acc(sh, sl, __ldg(Z + 2 * (int64_t)s));
             yv = vp_finish(sh, sl, Pv, n);
+        }
+        // edge points of C's edges {v, e_out(x)}, ids b..e-1: 0 + (p_v + FP(x))/4 + B[s]
+        const int64_t EPb = (int64_t)d.V + d.N1;
+        for (int s = b; s < e; ++s) {
+            const float4 ta = f4_mul(f4_add(Pv, __ldg(Z + 2 * (int64_t)s)), 0.25f);
+            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), __ldg(z.B + s)));
         }
     } else {
         // face points in column order, then the tails e_in(x) in ascending id
         float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
-#pragma unroll
-        for (int j = 0; j < U; ++j) if (j < n) { if (comp) dd_acc(sh, sl, fx[j]); else acc = f4_add(acc, fx[j]); }
-        for (int s = b + U; s < e; ++s) {
-            float4 f = ldg4(FP, __ldg(p.sc + s));
+        for (int s = b; s < e; ++s) {
+            const float4 f = __ldg(Z + 2 * (int64_t)s);
             if (comp) dd_acc(sh, sl, f); else acc = f4_add(acc, f);
         }
-        if (n <= U) {
-#pragma unroll
-            for (int r = 0; r < U; ++r) {
-#pragma unroll
-                for (int j = 0; j < U; ++j) {
-                    int rk = 0;
-#pragma unroll
-                    for (int i = 0; i < U; ++i) rk += (i < n) && tv[i] < tv[j];
-                    if (j < n && rk == r) { if (comp) dd_acc(sh, sl, pv[j]); else acc = f4_add(acc, pv[j]); }
-                }
+        int last = -1;
+        while (true) {
+            int xm = INT32_MAX, sm = -1;
+            for (int s = b; s < e; ++s) {
+                const int ti = __ldg(z.T + s);
+                if (ti > last && ti < xm) { xm = ti; sm = s; }
             }
-        } else {
-            int last = -1;
-            while (true) {
-                int xm = INT32_MAX;
-                for (int s = b; s < e; ++s) {
-                    int ti = __ldg(ids + 4 * __ldg(p.sc + s) + 3);
-                    if (ti > last && ti < xm) xm = ti;
-                }
-                if (xm == INT32_MAX) break;
-                if (comp) dd_acc(sh, sl, ldg4(P, xm)); else acc = f4_add(acc, ldg4(P, xm));
-                last = xm;
-            }
+            if (sm < 0) break;
+            const float4 pt = __ldg(Z + 2 * (int64_t)sm + 1);
+            if (comp) dd_acc(sh, sl, pt); else acc = f4_add(acc, pt);
+            last = xm;
         }
         if (comp) yv = vp_finish(sh, sl, Pv, n);
         else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
     }
     st4(R, v, yv);
     if (STATE) c.sptr[v] = b;
-}
-
-// G3e: one thread per slot s of P (corner x = sc1[s] of vertex v): C's edge
-// {v, e_out(x)} has id s in SLAK order; its edge point and state are written
-// at s (coalesced).  LAK only copies the column entry.
-template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g3e(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
-                                                QState p, QState c, float* __restrict__ R)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= d.N1) return;
-    const int x = __ldg(p.sc + s);
-    if (STATE) c.sc[s] = 4 * x;
-    if (LAK) return;
-    const int2 ve = __ldg(reinterpret_cast<const int2*>(ids) + 2 * x);      // {v, e_out(x)} of quad x
-    const int tw = __ldg(p.tw + x);
-    const float* FP = R + 4 * (int64_t)d.V;
-    float4 ta = f4_mul(f4_add(ldg4(P, ve.x), ldg4(FP, x)), 0.25f);
-    float4 tb = f4_mul(f4_add(ldg4(P, ve.y), ldg4(FP, qnext(tw))), 0.25f);
-    st4_cs(R, (int64_t)d.V + d.N1 + s, f4_add(f4_add(f4_zero(), ta), tb));
-    if (STATE) c.H[s] = make_int2(4 * x, 4 * qnext(tw) + 3);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <new>
 #include <vector>
+#include <algorithm>
 
 #include "common.cuh"
 #include "general.cuh"
@@ -35,6 +36,7 @@ struct Level {
     bool export_state = false;   // general level whose state feeds a fast level
     bool make_state = false;     // fast level whose state feeds the next fast level
     QState in_state{}, out_state{};
+    SlotScratch slots{};    // fast level: slot-ordered records from k_g1 to k_g3
     const int* ptr = nullptr;
     const int* ids = nullptr;
     const float* verts = nullptr;
@@ -130,7 +132,10 @@ struct slak_plan {
     DevStatus* h_st = nullptr;       // pinned
     int64_t maxN = 0, maxV = 0, maxE = 0;
     bool any_poly = false;
+    int64_t exN = 0, stN = 0, stV = 0, stE = 0, slN = 0, mid_ids = 0, mid_verts = 0;
+    bool arena_owned = true;
     QState qs[2]{};
+    SlotScratch slots{};
     // graph
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t gstream = nullptr;
@@ -289,17 +294,13 @@ void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
     const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
     k_g1<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
-                                                         reinterpret_cast<int4*>(L.o_ids), L.o_verts);
+                                                         reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots);
     lc.after("k_g1", 1, g1b);
     k_g2<LAK, STATE><<<grid_for(Pl.E), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
     lc.after("k_g2", 1, g2b);
-    k_g3v<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
-                                                              L.o_verts, comp ? 1 : 0);
-    lc.after("k_g3v", 1, 16 * Pl.V);
-    if (!LAK || STATE) {
-        k_g3e<LAK, STATE><<<grid_for(Pl.N), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
-        lc.after("k_g3e", 1, LAK ? 0 : 16 * L.F);
-    }
+    k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
+                                                             L.o_verts, comp ? 1 : 0);
+    lc.after("k_g3", 1, 16 * Pl.V + (LAK ? 0 : 16 * L.F));
 }
 
 void launch_fast(const Level& Pl, const Level& L, int scheme, bool comp, Lc& lc)
@@ -370,7 +371,7 @@ void free_plan_memory(slak_plan* p)
     p->ev.clear();
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     p->gexec = nullptr;
-    if (p->arena) cudaFree(p->arena);
+    if (p->arena && p->arena_owned) cudaFree(p->arena);
     p->arena = nullptr;
     if (p->h_st) cudaFreeHost(p->h_st);
     p->h_st = nullptr;
@@ -413,6 +414,148 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str)
     return SLAK_OK;
 }
 
+
+int validate_mesh(const slak_mesh* cm, int scheme)
+{
+    if (scheme != SLAK_SCHEME_LAK && scheme != SLAK_SCHEME_SLAK) return SLAK_ERR_INVALID_ARG;
+    if (cm->nfaces < 0 || cm->nverts < 0 || cm->nnz < 0) return SLAK_ERR_INVALID_ARG;
+    if (cm->type < SLAK_MESH_TRI || cm->type > SLAK_MESH_POLY) return SLAK_ERR_INVALID_ARG;
+    const bool quad_in = cm->type == SLAK_MESH_QUAD;
+    if (cm->nfaces > 0 && (!cm->ids || !cm->verts)) return SLAK_ERR_INVALID_ARG;
+    if (!quad_in && cm->nfaces > 0 && !cm->ptr) return SLAK_ERR_INVALID_ARG;
+    if (quad_in && cm->nnz != 4 * cm->nfaces) return SLAK_ERR_BAD_MESH;
+    if (cm->nnz >= (1ll << 31) || cm->nverts >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
+    return SLAK_OK;
+}
+
+// Level count and level-0 description (subdivideIteratively's rule: a
+// non-QUAD input always runs one polygon level).
+int plan_init(slak_plan* p, const slak_mesh* cm, int target_level, int scheme, int flags)
+{
+    p->scheme = scheme;
+    p->flags = flags;
+    const char* dbg = std::getenv("SLAK_DEBUG_SYNC");
+    p->debug = dbg && dbg[0] == '1';
+    p->in = *cm;
+    const bool quad_in = cm->type == SLAK_MESH_QUAD;
+    int nlev = quad_in ? 0 : 1;
+    if (target_level > nlev) nlev = target_level;
+    if (cm->nfaces == 0) nlev = 0;
+    p->lv.assign(nlev, Level{});
+    if (nlev) {
+        Level& L0 = p->lv[0];
+        L0.F = cm->nfaces; L0.V = cm->nverts; L0.N = cm->nnz;
+        L0.quad = quad_in;
+        L0.poly_fn = !quad_in;
+        L0.ptr = cm->ptr; L0.ids = cm->ids; L0.verts = cm->verts;
+    }
+    return nlev;
+}
+
+// All level sizes from level 0's boundary and edge counts; which levels run
+// closed-form; the maxima the arena is carved for.
+int plan_levels(slak_plan* p)
+{
+    const int nlev = (int)p->lv.size();
+    const bool force_general = (p->flags & SLAK_PLAN_GENERAL) != 0;
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (i > 0) {
+            const Level& P = p->lv[i - 1];
+            L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
+            L.E = (L.N - L.B) / 2 + L.B;
+            L.quad = true; L.poly_fn = false;
+            L.fast = !force_general && P.quad && P.B == 0;
+        }
+        L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
+        if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
+        if (!L.fast) {
+            if (L.N > p->maxN) p->maxN = L.N;
+            if (L.V > p->maxV) p->maxV = L.V;
+            if (L.E > p->maxE) p->maxE = L.E;
+            if (!L.quad) p->any_poly = true;
+        }
+    }
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (L.fast && p->lv[i - 1].N > p->slN) p->slN = p->lv[i - 1].N;
+        if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) { L.export_state = true; if (L.N > p->exN) p->exN = L.N; }
+        if (L.fast && i + 1 < nlev && p->lv[i + 1].fast) {
+            L.make_state = true;
+            if (L.N > p->stN) p->stN = L.N;
+            if (L.V > p->stV) p->stV = L.V;
+            if (L.E > p->stE) p->stE = L.E;
+        }
+    }
+    for (int i = 0; i + 1 < nlev; ++i) {
+        if (p->lv[i].No > p->mid_ids) p->mid_ids = p->lv[i].No;
+        if (p->lv[i].Vo > p->mid_verts) p->mid_verts = p->lv[i].Vo;
+    }
+    return SLAK_OK;
+}
+
+// Arena layout: general scratch, state export, fast-path states, slot records,
+// ping-pong intermediate meshes, status.  A dry Carver (null base) measures it.
+void plan_carve(slak_plan* p, Carver& cv)
+{
+    const int nlev = (int)p->lv.size();
+    carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
+    if (p->exN) carve_export(cv, p->s, p->exN);
+    if (p->stN) { carve_state(cv, p->qs[0], p->stN, p->stV, p->stE); carve_state(cv, p->qs[1], p->stN, p->stV, p->stE); }
+    if (p->slN) {
+        p->slots.Z = cv.take<float4>(2 * p->slN);
+        p->slots.B = cv.take<float4>(p->slN);
+        p->slots.T = cv.take<int>(p->slN);
+    }
+    for (int k = 0; k < 2; ++k) {
+        p->ping_ids[k] = nlev > 1 ? cv.take<int>(p->mid_ids) : nullptr;
+        p->ping_verts[k] = nlev > 1 ? cv.take<float>(4 * p->mid_verts) : nullptr;
+    }
+    p->st = cv.take<DevStatus>(1);
+}
+
+// Counts and flags of the refined mesh (arrays not set).
+slak_mesh plan_output_shape(const slak_plan* p)
+{
+    slak_mesh o{};
+    const Level& LL = p->lv.back();
+    o.type = SLAK_MESH_QUAD;
+    o.nfaces = LL.Fo; o.nnz = LL.No; o.nverts = LL.Vo;
+    if (p->scheme == SLAK_SCHEME_LAK) { o.max_face_order = 4; o.is_reduced = 0; }
+    else { o.max_face_order = 0; o.is_reduced = 1; }
+    return o;
+}
+
+// Level inputs/outputs and fast-path state wiring, once p->out holds the final arrays.
+void plan_wire(slak_plan* p)
+{
+    const int nlev = (int)p->lv.size();
+    for (int i = 0; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (i > 0) {
+            L.ids = p->lv[i - 1].o_ids;
+            L.verts = p->lv[i - 1].o_verts;
+            L.ptr = nullptr;
+        }
+        if (i == nlev - 1) {
+            L.o_ids = p->out.ids; L.o_verts = p->out.verts;
+            L.o_ptr = p->out.ptr; L.o_vals = p->out.vals;
+        } else {
+            L.o_ids = p->ping_ids[i & 1]; L.o_verts = p->ping_verts[i & 1];
+        }
+    }
+    int qi = 0;
+    for (int i = 1; i < nlev; ++i) {
+        Level& L = p->lv[i];
+        if (!L.fast) continue;
+        const Level& P = p->lv[i - 1];
+        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.sc, p->s.xslot, p->s.xtw, p->s.xt, p->s.H};
+        else L.in_state = P.out_state;
+        if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
+        L.slots = p->slots;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -441,130 +584,35 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
 {
     if (!cm || !out_plan) return SLAK_ERR_INVALID_ARG;
     *out_plan = nullptr;
-    if (scheme != SLAK_SCHEME_LAK && scheme != SLAK_SCHEME_SLAK) return SLAK_ERR_INVALID_ARG;
-    if (cm->nfaces < 0 || cm->nverts < 0 || cm->nnz < 0) return SLAK_ERR_INVALID_ARG;
-    if (cm->type < SLAK_MESH_TRI || cm->type > SLAK_MESH_POLY) return SLAK_ERR_INVALID_ARG;
-    const bool quad_in = cm->type == SLAK_MESH_QUAD;
-    if (cm->nfaces > 0 && (!cm->ids || !cm->verts)) return SLAK_ERR_INVALID_ARG;
-    if (!quad_in && cm->nfaces > 0 && !cm->ptr) return SLAK_ERR_INVALID_ARG;
-    if (quad_in && cm->nnz != 4 * cm->nfaces) return SLAK_ERR_BAD_MESH;
-    if (cm->nnz >= (1ll << 31) || cm->nverts >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
-
+    int rc = validate_mesh(cm, scheme);
+    if (rc != SLAK_OK) return rc;
     slak_plan* p = new (std::nothrow) slak_plan();
     if (!p) return SLAK_ERR_OOM;
-    p->scheme = scheme;
-    p->flags = flags;
-    {
-        const char* dbg = std::getenv("SLAK_DEBUG_SYNC");
-        p->debug = dbg && dbg[0] == '1';
-    }
-    p->in = *cm;
     cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
-    int nlev = (quad_in ? 0 : 1);
-    if (target_level > nlev) nlev = target_level;
-    if (cm->nfaces == 0) nlev = 0;
+    const int nlev = plan_init(p, cm, target_level, scheme, flags);
     cudaError_t ce = cudaMallocHost(&p->h_st, sizeof(DevStatus));
     if (ce != cudaSuccess) { delete p; return cuda_status(ce); }
     if (nlev == 0) { *out_plan = p; return SLAK_OK; }
-
-    // level geometry
-    p->lv.resize(nlev);
-    Level& L0 = p->lv[0];
-    L0.F = cm->nfaces; L0.V = cm->nverts; L0.N = cm->nnz;
-    L0.quad = quad_in;
-    L0.poly_fn = !quad_in;
-    L0.ptr = cm->ptr; L0.ids = cm->ids; L0.verts = cm->verts;
-    int rc = probe_level0(p, L0, str);
+    rc = probe_level0(p, p->lv[0], str);
+    if (rc == SLAK_OK) rc = plan_levels(p);
     if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
-    const bool force_general = (flags & SLAK_PLAN_GENERAL) != 0;
-    for (int i = 0; i < nlev; ++i) {
-        Level& L = p->lv[i];
-        if (i > 0) {
-            const Level& P = p->lv[i - 1];
-            L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
-            L.E = (L.N - L.B) / 2 + L.B;
-            L.quad = true; L.poly_fn = false;
-            L.fast = !force_general && P.quad && P.B == 0;
-        }
-        L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
-        if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) { free_plan_memory(p); delete p; return SLAK_ERR_UNSUPPORTED; }
-        if (!L.fast) {
-            if (L.N > p->maxN) p->maxN = L.N;
-            if (L.V > p->maxV) p->maxV = L.V;
-            if (L.E > p->maxE) p->maxE = L.E;
-            if (!L.quad) p->any_poly = true;
-        }
-    }
-    int64_t exN = 0, stN = 0, stV = 0, stE = 0;
-    for (int i = 0; i < nlev; ++i) {
-        Level& L = p->lv[i];
-        if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) { L.export_state = true; if (L.N > exN) exN = L.N; }
-        if (L.fast && i + 1 < nlev && p->lv[i + 1].fast) {
-            L.make_state = true;
-            if (L.N > stN) stN = L.N;
-            if (L.V > stV) stV = L.V;
-            if (L.E > stE) stE = L.E;
-        }
-    }
-    // arena: scratch + ping-pong intermediates + status
-    int64_t mid_ids = 0, mid_verts = 0;
-    for (int i = 0; i + 1 < nlev; ++i) {
-        if (p->lv[i].No > mid_ids) mid_ids = p->lv[i].No;
-        if (p->lv[i].Vo > mid_verts) mid_verts = p->lv[i].Vo;
-    }
-    auto carve_all = [&](Carver& cv) {
-        carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
-        if (exN) carve_export(cv, p->s, exN);
-        if (stN) { carve_state(cv, p->qs[0], stN, stV, stE); carve_state(cv, p->qs[1], stN, stV, stE); }
-        for (int k = 0; k < 2; ++k) {
-            p->ping_ids[k] = nlev > 1 ? cv.take<int>(mid_ids) : nullptr;
-            p->ping_verts[k] = nlev > 1 ? cv.take<float>(4 * mid_verts) : nullptr;
-        }
-        p->st = cv.take<DevStatus>(1);
-    };
     Carver dry(nullptr);
-    carve_all(dry);
+    plan_carve(p, dry);
     ce = cudaMalloc(&p->arena, dry.off);
     if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
     Carver cv((char*)p->arena);
-    carve_all(cv);
+    plan_carve(p, cv);
     // final outputs (caller-ownable, one allocation each)
-    const Level& LL = p->lv[nlev - 1];
-    p->out.type = SLAK_MESH_QUAD;
-    p->out.nfaces = LL.Fo; p->out.nnz = LL.No; p->out.nverts = LL.Vo;
-    ce = cudaMalloc(&p->out.ids, sizeof(int) * (size_t)LL.No);
-    if (ce == cudaSuccess) ce = cudaMalloc(&p->out.verts, sizeof(float) * 4 * (size_t)LL.Vo);
+    slak_mesh o = plan_output_shape(p);
+    ce = cudaMalloc(&o.ids, sizeof(int) * (size_t)o.nnz);
+    if (ce == cudaSuccess) ce = cudaMalloc(&o.verts, sizeof(float) * 4 * (size_t)o.nverts);
     if (ce == cudaSuccess && scheme == SLAK_SCHEME_LAK) {
-        ce = cudaMalloc(&p->out.ptr, sizeof(int) * (size_t)(LL.Fo + 1));
-        if (ce == cudaSuccess) ce = cudaMalloc(&p->out.vals, sizeof(int) * (size_t)LL.No);
+        ce = cudaMalloc(&o.ptr, sizeof(int) * (size_t)(o.nfaces + 1));
+        if (ce == cudaSuccess) ce = cudaMalloc(&o.vals, sizeof(int) * (size_t)o.nnz);
     }
+    p->out = o;
     if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
-    if (scheme == SLAK_SCHEME_LAK) { p->out.max_face_order = 4; p->out.is_reduced = 0; }
-    else { p->out.max_face_order = 0; p->out.is_reduced = 1; }
-    // wire level inputs / outputs
-    for (int i = 0; i < nlev; ++i) {
-        Level& L = p->lv[i];
-        if (i > 0) {
-            L.ids = p->lv[i - 1].o_ids;
-            L.verts = p->lv[i - 1].o_verts;
-            L.ptr = nullptr;
-        }
-        if (i == nlev - 1) {
-            L.o_ids = p->out.ids; L.o_verts = p->out.verts;
-            L.o_ptr = p->out.ptr; L.o_vals = p->out.vals;
-        } else {
-            L.o_ids = p->ping_ids[i & 1]; L.o_verts = p->ping_verts[i & 1];
-        }
-    }
-    int qi = 0;
-    for (int i = 1; i < nlev; ++i) {
-        Level& L = p->lv[i];
-        if (!L.fast) continue;
-        const Level& P = p->lv[i - 1];
-        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.sc, p->s.xslot, p->s.xtw, p->s.xt, p->s.H};
-        else L.in_state = P.out_state;
-        if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
-    }
+    plan_wire(p);
     *out_plan = p;
     return SLAK_OK;
 }
@@ -700,6 +748,310 @@ int slak_mesh_free(slak_mesh* m)
     if (m->verts) { t = cudaFree(m->verts); if (t != cudaSuccess) e = t; }
     std::memset(m, 0, sizeof(*m));
     return cuda_status(e);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batches: many meshes, each with its own level count, refined by one call.
+//
+// Every mesh gets its own plan (so each mesh's numbering and float results are
+// exactly those of slak_subdivide on it alone), but all plans are sized up
+// front, share one device arena per wave and write straight into one batch
+// output buffer.  Within a wave, meshes are dealt round-robin onto parallel
+// streams, so small meshes run concurrently; waves reuse the arena in turn.
+// With SLAK_PLAN_GRAPH the whole batch (every wave, mesh and level) is captured
+// as one CUDA graph whose branches are the per-mesh level chains.
+struct slak_batch {
+    int scheme = SLAK_SCHEME_SLAK;
+    int flags = 0;
+    std::vector<slak_plan*> plans;              // nullptr where the mesh is not refined
+    std::vector<slak_mesh> outs;
+    std::vector<std::vector<int64_t>> waves;    // mesh indices per wave
+    void* out_mem = nullptr;
+    void* arena = nullptr;
+    size_t out_bytes = 0, arena_bytes = 0;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> fork, join;
+    cudaGraphExec_t gexec = nullptr;
+    DevStatus* h_st = nullptr;                  // pinned, one per mesh
+    int64_t launches = 0;
+    int executed = 0;
+};
+
+namespace {
+
+constexpr int kBatchStreams = 16;
+
+void batch_free(slak_batch* b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    for (auto* p : b->plans)
+        if (p) { free_plan_memory(p); delete p; }
+    for (auto s : b->streams) cudaStreamDestroy(s);
+    for (auto e : b->fork) cudaEventDestroy(e);
+    for (auto e : b->join) cudaEventDestroy(e);
+    if (b->out_mem) cudaFree(b->out_mem);
+    if (b->arena) cudaFree(b->arena);
+    if (b->h_st) cudaFreeHost(b->h_st);
+    delete b;
+}
+
+size_t out_bytes_of(const slak_mesh& o, bool lak)
+{
+    size_t b = align_up(sizeof(int) * (size_t)o.nnz) + align_up(sizeof(float) * 4 * (size_t)o.nverts);
+    if (lak) b += align_up(sizeof(int) * (size_t)(o.nfaces + 1)) + align_up(sizeof(int) * (size_t)o.nnz);
+    return b;
+}
+
+int batch_enqueue(slak_batch* b, cudaStream_t str)
+{
+    int64_t nl = 0;
+    for (size_t w = 0; w < b->waves.size(); ++w) {
+        const auto& wave = b->waves[w];
+        const int nb = (int)std::min<size_t>(kBatchStreams, wave.size());
+        cudaEventRecord(b->fork[w], str);
+        for (int k = 0; k < nb; ++k) cudaStreamWaitEvent(b->streams[k], b->fork[w], 0);
+        for (size_t j = 0; j < wave.size(); ++j) {
+            slak_plan* p = b->plans[wave[j]];
+            int rc = enqueue_all(p, b->streams[j % nb]);
+            if (rc != SLAK_OK) return rc;
+            nl += p->launches;
+        }
+        for (int k = 0; k < nb; ++k) {
+            cudaEventRecord(b->join[w * kBatchStreams + k], b->streams[k]);
+            cudaStreamWaitEvent(str, b->join[w * kBatchStreams + k], 0);
+        }
+    }
+    b->launches = nl;
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
+                      slak_stream_t stream, slak_batch** out_batch)
+{
+    if (!meshes || !levels || count < 0 || !out_batch) return SLAK_ERR_INVALID_ARG;
+    *out_batch = nullptr;
+    slak_batch* b = new (std::nothrow) slak_batch();
+    if (!b) return SLAK_ERR_OOM;
+    b->scheme = scheme;
+    b->flags = flags;
+    b->plans.assign(count, nullptr);
+    b->outs.assign(count, slak_mesh{});
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    int rc = SLAK_OK;
+    int64_t maxN = 0, maxV = 0;
+    bool any_poly = false;
+    for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+        rc = validate_mesh(&meshes[i], scheme);
+        if (rc != SLAK_OK) break;
+        slak_plan* p = new (std::nothrow) slak_plan();
+        if (!p) { rc = SLAK_ERR_OOM; break; }
+        p->arena_owned = false;
+        p->out_owned = false;
+        b->plans[i] = p;
+        if (plan_init(p, &meshes[i], levels[i], scheme, flags & ~SLAK_PLAN_GRAPH) == 0) {
+            delete p;
+            b->plans[i] = nullptr;
+            continue;
+        }
+        maxN = std::max(maxN, meshes[i].nnz);
+        maxV = std::max(maxV, meshes[i].nverts);
+        any_poly |= meshes[i].type != SLAK_MESH_QUAD;
+    }
+    cudaError_t ce = cudaSuccess;
+    if (rc == SLAK_OK) ce = cudaMallocHost(&b->h_st, sizeof(DevStatus) * (size_t)(count > 0 ? count : 1));
+    if (rc == SLAK_OK && ce != cudaSuccess) rc = cuda_status(ce);
+    // level-0 topology of every mesh: one scratch, results copied back in stream order, one sync
+    if (rc == SLAK_OK && maxN > 0) {
+        Carver dry(nullptr);
+        Scratch sc;
+        carve_scratch(dry, sc, maxN, maxV, 1, any_poly);
+        DevStatus* st = dry.take<DevStatus>(1);
+        void* mem = nullptr;
+        ce = cudaMalloc(&mem, dry.off);
+        if (ce != cudaSuccess) rc = cuda_status(ce);
+        else {
+            Carver cv((char*)mem);
+            carve_scratch(cv, sc, maxN, maxV, 1, any_poly);
+            st = cv.take<DevStatus>(1);
+            int64_t nl = 0;
+            Lc lc{str, &nl, false, 0};
+            for (int64_t i = 0; i < count; ++i) {
+                slak_plan* p = b->plans[i];
+                if (!p) continue;
+                cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
+                launch_topology_a(p->lv[0], 0, scheme, sc, st, lc);
+                cudaMemcpyAsync(&b->h_st[i], st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+                cudaMemcpyAsync(&b->h_st[i].nedges, sc.eptr + p->lv[0].V, sizeof(int), cudaMemcpyDeviceToHost, str);
+            }
+            ce = cudaStreamSynchronize(str);
+            cudaFree(mem);
+            if (ce != cudaSuccess) rc = cuda_status(ce);
+        }
+        for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+            slak_plan* p = b->plans[i];
+            if (!p) continue;
+            if (b->h_st[i].err) {
+                g_detail = "mesh " + std::to_string(i) + ": device detail " + std::to_string(b->h_st[i].detail);
+                rc = b->h_st[i].err;
+                break;
+            }
+            Level& L0 = p->lv[0];
+            L0.B = b->h_st[i].bcount[0];
+            L0.E = b->h_st[i].nedges;
+            if (L0.E != (L0.N - L0.B) / 2 + L0.B) { g_detail = "mesh " + std::to_string(i); rc = SLAK_ERR_BAD_MESH; }
+            else rc = plan_levels(p);
+        }
+    }
+    // memory: every mesh's output in one buffer; waves of plans sharing one arena
+    std::vector<size_t> ab(count, 0), ob(count, 0);
+    size_t total_out = 0;
+    for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+        slak_plan* p = b->plans[i];
+        if (!p) continue;
+        Carver dry(nullptr);
+        plan_carve(p, dry);
+        ab[i] = dry.off;
+        b->outs[i] = plan_output_shape(p);
+        ob[i] = out_bytes_of(b->outs[i], scheme == SLAK_SCHEME_LAK);
+        total_out += ob[i];
+    }
+    if (rc == SLAK_OK) {
+        size_t freeb = 0, totalb = 0;
+        cudaMemGetInfo(&freeb, &totalb);
+        const size_t margin = size_t(2) << 30;
+        if (total_out + margin > freeb) { g_detail = "batch outputs exceed device memory"; rc = SLAK_ERR_OOM; }
+        size_t budget = rc == SLAK_OK ? (freeb - total_out - margin) * 3 / 4 : 0;
+        size_t cap = size_t(24) << 30;
+        if (const char* wb = std::getenv("SLAK_BATCH_WAVE_BYTES")) cap = (size_t)std::strtoull(wb, nullptr, 10);
+        if (budget > cap) budget = cap;
+        // greedy waves in mesh order
+        std::vector<int64_t> cur;
+        size_t cur_b = 0;
+        for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+            if (!b->plans[i]) continue;
+            if (ab[i] > budget) { g_detail = "mesh " + std::to_string(i) + " needs more scratch than is free"; rc = SLAK_ERR_OOM; break; }
+            if (cur_b + ab[i] > budget && !cur.empty()) {
+                b->waves.push_back(cur);
+                b->arena_bytes = std::max(b->arena_bytes, cur_b);
+                cur.clear();
+                cur_b = 0;
+            }
+            cur.push_back(i);
+            cur_b += ab[i];
+        }
+        if (!cur.empty()) { b->waves.push_back(cur); b->arena_bytes = std::max(b->arena_bytes, cur_b); }
+    }
+    if (rc == SLAK_OK && total_out) {
+        ce = cudaMalloc(&b->out_mem, total_out);
+        if (ce == cudaSuccess && b->arena_bytes) ce = cudaMalloc(&b->arena, b->arena_bytes);
+        if (ce != cudaSuccess) rc = cuda_status(ce);
+    }
+    if (rc == SLAK_OK) {
+        char* o = static_cast<char*>(b->out_mem);
+        for (int64_t i = 0; i < count; ++i) {
+            if (!b->plans[i]) continue;
+            slak_mesh& m = b->outs[i];
+            m.ids = reinterpret_cast<int*>(o); o += align_up(sizeof(int) * (size_t)m.nnz);
+            m.verts = reinterpret_cast<float*>(o); o += align_up(sizeof(float) * 4 * (size_t)m.nverts);
+            if (scheme == SLAK_SCHEME_LAK) {
+                m.ptr = reinterpret_cast<int*>(o); o += align_up(sizeof(int) * (size_t)(m.nfaces + 1));
+                m.vals = reinterpret_cast<int*>(o); o += align_up(sizeof(int) * (size_t)m.nnz);
+            }
+        }
+        for (const auto& wave : b->waves) {
+            size_t off = 0;
+            for (int64_t i : wave) {
+                slak_plan* p = b->plans[i];
+                p->arena = static_cast<char*>(b->arena) + off;
+                Carver cv(static_cast<char*>(p->arena));
+                plan_carve(p, cv);
+                off += ab[i];
+                p->out = b->outs[i];
+                plan_wire(p);
+            }
+        }
+        b->fork.resize(b->waves.size());
+        b->join.resize(b->waves.size() * kBatchStreams);
+        for (auto& e : b->fork) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        for (auto& e : b->join) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        b->streams.resize(kBatchStreams);
+        for (auto& st2 : b->streams) cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+        ce = cudaGetLastError();
+        if (ce != cudaSuccess) rc = cuda_status(ce);
+    }
+    if (rc != SLAK_OK) { batch_free(b); return rc; }
+    *out_batch = b;
+    return SLAK_OK;
+}
+
+int slak_batch_execute(slak_batch* b, slak_stream_t stream)
+{
+    if (!b) return SLAK_ERR_INVALID_ARG;
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    int rc;
+    if ((b->flags & SLAK_PLAN_GRAPH) && str != nullptr) {
+        if (!b->gexec) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(str, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_status(e);
+            rc = batch_enqueue(b, str);
+            e = cudaStreamEndCapture(str, &g);
+            if (rc != SLAK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+            if (e != cudaSuccess) return cuda_status(e);
+            e = cudaGraphInstantiate(&b->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        rc = cuda_status(cudaGraphLaunch(b->gexec, str));
+    } else {
+        rc = batch_enqueue(b, str);
+    }
+    b->executed = 1;
+    for (auto* p : b->plans) if (p) p->executed = 1;
+    return rc;
+}
+
+int slak_batch_status(slak_batch* b, slak_stream_t stream)
+{
+    if (!b) return SLAK_ERR_INVALID_ARG;
+    if (!b->executed) return SLAK_ERR_NOT_READY;
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) { g_detail = std::string("batch: ") + cudaGetErrorString(e); return cuda_status(e); }
+    for (size_t i = 0; i < b->plans.size(); ++i)
+        if (b->plans[i]) cudaMemcpyAsync(&b->h_st[i], b->plans[i]->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+    e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) return cuda_status(e);
+    for (size_t i = 0; i < b->plans.size(); ++i)
+        if (b->plans[i] && b->h_st[i].err) {
+            g_detail = "mesh " + std::to_string(i) + ": device detail " + std::to_string(b->h_st[i].detail);
+            return b->h_st[i].err;
+        }
+    return SLAK_OK;
+}
+
+int slak_batch_output(const slak_batch* b, int64_t index, slak_mesh* rmesh)
+{
+    if (!b || !rmesh || index < 0 || index >= (int64_t)b->outs.size()) return SLAK_ERR_INVALID_ARG;
+    if (!b->plans[index]) return SLAK_OK;     // nothing refined: *rmesh untouched
+    *rmesh = b->outs[index];
+    return SLAK_OK;
+}
+
+int slak_batch_num_waves(const slak_batch* b) { return b ? (int)b->waves.size() : 0; }
+
+int64_t slak_batch_launches(const slak_batch* b) { return b ? b->launches : 0; }
+
+int slak_batch_destroy(slak_batch* b)
+{
+    if (b) batch_free(b);
+    return SLAK_OK;
 }
 
 }  // extern "C"

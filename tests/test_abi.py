@@ -11,7 +11,7 @@ from slak_b200 import _abi, _paths
 def _declared():
     src = open(os.path.join(_paths.INCLUDE_DIR, "slak_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(slak_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(slak_[a-z_0-9]+)\s*\(", src)))
 
 
 @pytest.fixture(scope="module")
