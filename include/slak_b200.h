@@ -91,6 +91,36 @@ int slak_subdivide(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, i
 int slak_mesh_free(slak_mesh* mesh);
 
 /*
+ * One subdivision level that allocates no device memory.  No counterpart in the
+ * reference.  It is meant for callers that cannot call cudaMalloc: an
+ * application whose device memory is owned by its own pool allocator, or a
+ * latency-critical loop that must not hit cudaMalloc/cudaFree, since those can
+ * synchronise the device and take unbounded time.
+ *
+ * Runs the reference's first-level functions for a non-QUAD cmesh (the quad
+ * functions for a QUAD cmesh), exactly as slak_subdivide with target_level 1.
+ * The caller allocates the outputs:
+ *   rmesh->ids    4*nnz ints
+ *   rmesh->verts  4*rmesh->nverts floats; on entry rmesh->nverts is the buffer's
+ *                 capacity in vertices (nverts + nfaces + nnz always suffices)
+ *   rmesh->ptr, rmesh->vals   nnz+1 and 4*nnz ints, LAK only
+ * On success, the counts in *rmesh are set as slak_subdivide sets them.
+ *
+ * The scratch is a fixed 32 MiB device array inside this library.  Every GPU
+ * that loads the library holds it until the process exits.  Meshes whose
+ * scratch does not fit are rejected with SLAK_ERR_UNSUPPORTED (about
+ * 500k corners).  All calls share that array:
+ *   - calls that overlap on the GPU (two streams, or two host threads) race,
+ *     so serialise them;
+ *   - each call clears what must start at zero.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  The call waits for `stream` twice: for the level's edge
+ * count and for its status.
+ */
+int slak_subdivide_level_noalloc(const slak_mesh* cmesh, slak_mesh* rmesh, int scheme, slak_stream_t stream);
+
+/*
  * Plans: the same computation with every size fixed up front, all device
  * memory allocated at creation and nothing allocated or synchronised when it
  * runs, so one execution can be captured in a CUDA graph.  No reference

@@ -1055,3 +1055,110 @@ int slak_batch_destroy(slak_batch* b)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// One subdivision level that allocates nothing.  Some callers cannot call
+// cudaMalloc: an application whose device memory is owned by its own pool
+// allocator, or a latency-critical loop that must not hit cudaMalloc/cudaFree
+// (which can synchronise the device and take unbounded time).  For them the
+// scratch of one general level lives in a fixed, file-scope device array of
+// kNoAllocScratchBytes; the caller passes the input mesh and the output
+// buffers.  Every GPU that loads this library holds the array until exit.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;     // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int slak_subdivide_level_noalloc(const slak_mesh* cm, slak_mesh* rm, int scheme, slak_stream_t stream)
+{
+    if (!cm || !rm) return SLAK_ERR_INVALID_ARG;
+    if (scheme != SLAK_SCHEME_LAK && scheme != SLAK_SCHEME_SLAK) return SLAK_ERR_INVALID_ARG;
+    if (cm->type < SLAK_MESH_TRI || cm->type > SLAK_MESH_POLY) return SLAK_ERR_INVALID_ARG;
+    if (cm->nfaces <= 0 || cm->nverts <= 0 || cm->nnz <= 0 || !cm->ids || !cm->verts) return SLAK_ERR_INVALID_ARG;
+    const bool quad = cm->type == SLAK_MESH_QUAD, lak = scheme == SLAK_SCHEME_LAK;
+    if (quad && cm->nnz != 4 * cm->nfaces) return SLAK_ERR_BAD_MESH;
+    if (!quad && !cm->ptr) return SLAK_ERR_INVALID_ARG;
+    if (!rm->ids || !rm->verts || (lak && (!rm->ptr || !rm->vals))) return SLAK_ERR_INVALID_ARG;
+    if (4 * cm->nnz >= (1ll << 31) || cm->nverts >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
+
+    // the scratch of one general level (edges <= corners), checked against the fixed array
+    const int64_t N = cm->nnz, V = cm->nverts, F = cm->nfaces;
+    Scratch s;
+    Carver dry(nullptr);
+    carve_scratch(dry, s, N, V, N, !quad);
+    dry.take<DevStatus>(1);
+    if (dry.off > kNoAllocScratchBytes) {
+        g_detail = "mesh needs " + std::to_string(dry.off) + " bytes of scratch; the allocation-free entry point has " +
+                   std::to_string(kNoAllocScratchBytes);
+        return SLAK_ERR_UNSUPPORTED;
+    }
+
+    // device address of the array, looked up once per device with that device current
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= kMaxDevices) return SLAK_ERR_UNSUPPORTED;
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                g_detail = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return cuda_status(e);
+            }
+        }
+        base = g_noalloc_addr[dev];
+    }
+    Carver cv(static_cast<char*>(base));
+    carve_scratch(cv, s, N, V, N, !quad);
+    DevStatus* st = cv.take<DevStatus>(1);
+
+    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
+    Level L;
+    L.F = F; L.V = V; L.N = N;
+    L.quad = quad; L.poly_fn = !quad;
+    L.ptr = cm->ptr; L.ids = cm->ids; L.verts = cm->verts;
+    int64_t nl = 0;
+    Lc lc{str, &nl, false, 0};
+    cudaMemsetAsync(st, 0, sizeof(DevStatus), str);              // the array keeps the last call's contents
+    launch_topology_a(L, 0, scheme, s, st, lc);
+    DevStatus h;
+    int nedges = 0;
+    cudaMemcpyAsync(&h, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+    cudaMemcpyAsync(&nedges, s.eptr + V, sizeof(int), cudaMemcpyDeviceToHost, str);
+    e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (h.err) return h.err;
+    L.B = h.bcount[0];
+    L.E = nedges;
+    if (L.E != (N - L.B) / 2 + L.B) return SLAK_ERR_BAD_MESH;
+    L.Fo = N; L.No = 4 * N; L.Vo = V + F + L.E;
+    if (rm->nverts < L.Vo) {      // rm->nverts carries the capacity of rm->verts, in vertices
+        g_detail = "output positions need " + std::to_string(L.Vo) + " vertices";
+        return SLAK_ERR_INVALID_ARG;
+    }
+    L.o_ids = rm->ids; L.o_verts = rm->verts;
+    L.o_ptr = lak ? rm->ptr : nullptr;
+    L.o_vals = lak ? rm->vals : nullptr;
+    if (quad) launch_rest<true>(L, scheme, false, s, st, lc);
+    else launch_rest<false>(L, scheme, false, s, st, lc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    cudaMemcpyAsync(&h, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
+    e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (h.err) return h.err;
+    rm->type = SLAK_MESH_QUAD;
+    rm->nfaces = L.Fo; rm->nnz = L.No; rm->nverts = L.Vo;
+    rm->is_reduced = lak ? 0 : 1;
+    if (lak) rm->max_face_order = 4;
+    return SLAK_OK;
+}
