@@ -34,6 +34,12 @@ sys.path.insert(0, HERE)
 
 HBM_FALLBACK_GBS = 6650.0
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit of work of a
+# kernel, from one ncu capture of a smaller case of the same structure
+# (profiles/k_g_fast_levels_mixed384_slak.txt: k_g1 of the last level, SLAK,
+# per quad of the level it refines); scaled by the units of the bench's launch.
+TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 181.92}
+
 
 def _peaks():
     try:
@@ -102,7 +108,8 @@ def _max_over_ranks(dist, x: float) -> float:
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -176,6 +183,12 @@ def run_ours(args, dist, rank, ws):
 
     # dominant kernel: per-kernel events of instrumented eager executions
     kern, ktable = plan_kernel_profile(dm, levels, scheme, args.steps, stream, torch, flush)
+    tpu = TRAFFIC_PER_UNIT.get((kern["kernel"], args.scheme, "last" if kern["level"] == levels - 1 else "mid"))
+    if tpu is not None:
+        units = stats[kern["level"]]["nfaces"]
+        kern["traffic"] = tpu * units
+        kern["traffic_note"] = (f"{tpu} B per quad refined (ncu, mixed:384 capture) x {units} quads; "
+                                f"{tpu * units / kern['algorithmic_bytes_per_launch']:.2f}x the algorithmic bytes")
 
     # e2e: host buffers, the C-ABI drop-in call
     e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws)
@@ -283,14 +296,140 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
         out_ids.copy_(api.device_view(cout.ids, (cout.nnz,), "<i4"), non_blocking=True)
         out_verts.copy_(api.device_view(cout.verts, (4 * cout.nverts,), "<f4"), non_blocking=True)
         torch.cuda.synchronize()
-        faces = cout.nfaces
-        lib.slak_mesh_free(ctypes.byref(cout))
         dt = time.perf_counter() - t0
+        faces = cout.nfaces
+        lib.slak_mesh_free(ctypes.byref(cout))       # outside the bracket, as for the reference arm
         if i >= args.warmup:
             times.append(dt)
     t = _max_over_ranks(dist, statistics.mean(times))
     return {"value": faces * ws / t, "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3}
+
+
+def batch_shard(count, rank=0, ws=1):
+    """Specs of this rank's meshes of the 2,000-mesh batch (seeded kinds, sizes
+    and level counts): with ws > 1 each rank takes every ws-th mesh."""
+    from slak_b200 import meshgen
+    return [it for k, it in enumerate(meshgen.batch_specs(count)) if k % ws == rank]
+
+
+def batch_workload(count, rank=0, ws=1):
+    from slak_b200 import meshgen
+    return [(meshgen.batch_mesh(it), it.levels) for it in batch_shard(count, rank, ws)]
+
+
+def run_batch(args, torch, dist, rank, ws):
+    """Batched form vs the plain per-mesh loop on the same meshes.
+
+    plain   one slak_subdivide per mesh (the drop-in call, as a caller of the
+            reference loops over meshes), outputs freed after each call;
+            device-resident inputs; one CUDA-event bracket around the loop
+    batched one slak_batch_* object for all meshes, executed as one CUDA graph
+            (SLAK_PLAN_GRAPH); the inputs (1.7 GB) exceed L2, so no flush
+    """
+    import ctypes
+    from slak_b200 import _abi, api
+    from slak_b200.mesh import LAK, SLAK
+    scheme = SLAK if args.scheme == "slak" else LAK
+    t0 = time.perf_counter()
+    items = batch_workload(args.batch_count, rank, ws)
+    if scheme == LAK:
+        items = [(m if m.ptr is not None else m.with_quad_ptr(), l) for m, l in items]
+    gen_s = time.perf_counter() - t0
+    dms = [api.DeviceMesh.from_host(m) for m, _ in items]
+    stream = torch.cuda.Stream()
+    lib = _abi.lib()
+    sh = int(stream.cuda_stream)
+    cins = [d.as_c() for d in dms]
+
+    def plain_loop(count=None):
+        faces = 0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for cin, (_, lv) in list(zip(cins, items))[:count]:
+            cout = _abi.SlakMesh()
+            _abi.check(lib.slak_subdivide(ctypes.byref(cin), ctypes.byref(cout), lv, scheme, sh), "slak_subdivide")
+            faces += cout.nfaces
+            lib.slak_mesh_free(ctypes.byref(cout))
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), faces
+
+    def plan_loop():
+        # the same per-mesh loop with each mesh's plan created (and its memory
+        # allocated) outside the bracket: device time of the executions alone
+        total = 0.0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for d, (_, lv) in zip(dms, items):
+            p = api.Plan(d, lv, scheme, 0, stream=stream)
+            a.record(stream)
+            p.execute(stream)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+            p.check(stream)
+            p.close()
+        return total
+
+    with torch.cuda.stream(stream):
+        plain_loop(50)                                    # warm-up
+        plain = [plain_loop() for _ in range(max(1, args.batch_plain_reps))]
+        plan_ms = plan_loop()
+    plain_ms = _max_over_ranks(dist, statistics.mean(p[0] for p in plain))
+    plan_ms = _max_over_ranks(dist, plan_ms)
+    faces = plain[0][1]
+
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        b = api.Batch(dms, [l for _, l in items], scheme, api._abi.PLAN_GRAPH, stream=stream)
+    create_s = time.perf_counter() - t0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dev = torch.cuda.current_device()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            b.execute(stream)
+        b.check(stream)
+        torch.cuda.synchronize()
+        _barrier(dist)
+        with ClockSampler(dev) as clk:
+            for i in range(args.steps):
+                ev[i][0].record(stream)
+                b.execute(stream)
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        b.check(stream)
+    batch_ms = _max_over_ranks(dist, statistics.mean(a.elapsed_time(c) for a, c in ev))
+    out = {"meshes": len(items) * ws, "refined_faces": faces * ws,
+           "plain_ms": plain_ms, "plain_value": faces * ws / (plain_ms * 1e-3),
+           "batched_ms": batch_ms, "batched_value": faces * ws / (batch_ms * 1e-3),
+           "speedup": plain_ms / batch_ms, "unit": "refined_faces/s",
+           "plan_loop_ms": plan_ms, "plan_loop_value": faces * ws / (plan_ms * 1e-3),
+           "speedup_vs_plan_loop": plan_ms / batch_ms,
+           "waves": b.waves, "launches_per_execution": b.launches,
+           "create_s": create_s, "generate_s": gen_s, "clocks": clk.summary(),
+           "plain": "slak_subdivide per mesh (allocates and frees its output per call)",
+           "plan_loop": "per mesh: plan created untimed, one eager execution timed with CUDA events",
+           "batched": "slak_batch, one CUDA graph per execution"}
+    b.close()
+    return out
+
+
+def run_batch_line(args, dist, rank, ws):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    r = run_batch(args, torch, dist, rank, ws)
+    peak, peak_kind = _peaks()
+    return {
+        "metric": "refined_faces_per_s", "value": r["batched_value"], "unit": "refined_faces/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["batched_ms"], "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"batch{args.batch_count}: {r['meshes']} meshes, {args.scheme.upper()}, "
+                               f"levels 1-4 -> {r['refined_faces']} quads",
+                   "l2": "inputs 1.7 GB > L2", "parallelism": f"meshes split over {ws} ranks"},
+        "gpu_launches": r["launches_per_execution"] * args.steps,
+        "batched": r, "clocks": r["clocks"],
+    }
 
 
 def run_reference(args, dist, rank, ws):
@@ -311,6 +450,11 @@ def run_reference(args, dist, rank, ws):
     faces = sizes[-1][2]
     ms_step = statistics.mean(ms)
     value = faces / (ms_step * 1e-3)
+    # end to end through the reference's public call with host buffers: the
+    # same pinned H2D of the input and D2H of the refined ids and positions as
+    # this repository's e2e figure
+    e2e_ms, h2d, d2h = ref.time_e2e(mesh, levels, scheme, 1, max(2, min(args.steps, 5)))
+    e2e_t = statistics.mean(e2e_ms)
     return {
         "impl": "reference", "metric": "refined_faces_per_s", "value": value, "unit": "refined_faces/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -323,7 +467,8 @@ def run_reference(args, dist, rank, ws):
         "cpu_baseline": {"value": value, "unit": "refined_faces/s", "cores": 1, "kind": "reference",
                          "sample": "GPUPeople/SLAK's own CUDA path (built for sm_100a) on the full workload; "
                                    "the reference has no CPU implementation"},
-        "e2e": {"value": value, "unit": "refined_faces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": faces / (e2e_t * 1e-3), "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t},
         "clocks": clk.summary(),
     }
 
@@ -338,11 +483,15 @@ def main():
     ap.add_argument("--scheme", default="slak", choices=["slak", "lak"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--batch-count", type=int, default=2000)
+    ap.add_argument("--batch-plain-reps", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     dist, rank, ws = _dist()
     if args.impl == "reference":
         out = run_reference(args, dist, rank, ws)
+    elif args.workload == "batch2000":
+        out = run_batch_line(args, dist, rank, ws)
     else:
         out = run_ours(args, dist, rank, ws)
     if rank == 0 and out is not None:

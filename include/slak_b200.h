@@ -81,10 +81,19 @@ const char* slak_last_error_detail(void);
  * NULL, is_reduced = 1, max_face_order copied from the input; LAK output:
  * ptr[i] = 4i, vals[i] = i%4+1, max_face_order = 4, is_reduced = 0.
  * Work is ordered on `stream`; the call returns once the refined mesh is
- * complete (the reference is synchronous too).
+ * complete (the reference is synchronous too).  Intermediate levels live in a
+ * per-device workspace that is kept for the next call (the reference
+ * allocates and frees them inside every call); a call made while another
+ * holds the workspace allocates its own.  SLAK_WORKSPACE_CACHE=0 in the
+ * environment turns the cache off.
  */
 int slak_subdivide(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
                    slak_stream_t stream);
+
+/* Frees the current device's cached slak_subdivide workspace.  No counterpart
+ * in the reference, whose calls keep nothing between them.  Returns
+ * SLAK_ERR_NOT_READY while a call holds the workspace. */
+int slak_workspace_release(void);
 
 /* cudaFree of every non-NULL array, then zero the descriptor
  * (MeshInfo::freeAndReset, CatmullClark.h:99-106). */

@@ -40,6 +40,10 @@ def lib():
         L.ref_run.argtypes = [ctypes.c_int, P, ctypes.c_int, P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
         L.ref_time.argtypes = [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+        L.ref_time_e2e.argtypes = [ctypes.c_int, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+        L.ref_time_e2e.restype = ctypes.c_int
         L.ref_free.argtypes = [P]
         L.ref_run.restype = L.ref_time.restype = ctypes.c_int
         _lib = L
@@ -101,3 +105,18 @@ def time(mesh, levels: int, scheme: int, warmup: int, reps: int, quiet: bool = T
     if rc != 0:
         raise RuntimeError(f"reference timing failed with code {rc}")
     return list(ms), list(self_ms)
+
+
+def time_e2e(mesh, levels: int, scheme: int, warmup: int, reps: int, quiet: bool = True):
+    """Per-call wall time (ms) with host buffers: pinned H2D of the input,
+    subdivideIteratively, D2H of the refined ids and positions.  Returns
+    (ms list, h2d bytes, d2h bytes)."""
+    keep = []
+    cin = _in(mesh, keep)
+    ms = (ctypes.c_double * reps)()
+    hb, db = ctypes.c_int64(0), ctypes.c_int64(0)
+    rc = lib().ref_time_e2e(scheme, ctypes.byref(cin), levels, warmup, reps, ms, ctypes.byref(hb),
+                            ctypes.byref(db), int(quiet))
+    if rc != 0:
+        raise RuntimeError(f"reference end-to-end timing failed with code {rc}")
+    return list(ms), int(hb.value), int(db.value)

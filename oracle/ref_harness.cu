@@ -6,6 +6,8 @@
 #include "CatmullClark.h"
 #include "LAKCatmullClark.h"
 
+#include <chrono>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -209,6 +211,69 @@ int ref_time(int scheme, const ref_mesh* in, int levels, int warmup, int reps, d
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    return rc;
+}
+
+// End-to-end time of `reps` calls with host buffers (ms_each, wall clock):
+// per call, the input is copied from pinned host memory into the device
+// arrays, subdivideIteratively runs, and the refined ids and positions are
+// copied back into pinned host memory; the output is freed outside the bracket.
+int ref_time_e2e(int scheme, const ref_mesh* in, int levels, int warmup, int reps, double* ms_each,
+                 int64_t* h2d_bytes, int64_t* d2h_bytes, int quiet)
+{
+    DevInput d;
+    int rc = d.upload(*in);
+    if (rc) return rc;
+    const size_t bp = in->ptr ? sizeof(int) * (in->nfaces + 1) : 0, bi = sizeof(int) * in->nnz;
+    const size_t bv = in->vals ? sizeof(int) * in->nnz : 0, bx = sizeof(float) * 4 * in->nverts;
+    char* hin = nullptr;
+    if (cudaMallocHost(&hin, bp + bi + bv + bx) != cudaSuccess) return 3;
+    if (bp) std::memcpy(hin, in->ptr, bp);
+    std::memcpy(hin + bp, in->ids, bi);
+    if (bv) std::memcpy(hin + bp + bi, in->vals, bv);
+    std::memcpy(hin + bp + bi + bv, in->verts, bx);
+    char* hout = nullptr;
+    size_t out_cap = 0;
+    *h2d_bytes = (int64_t)(bp + bi + bv + bx);
+    StdoutCapture cap(quiet != 0);
+    for (int i = -warmup; i < reps && !rc; ++i) {
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        if (bp) cudaMemcpyAsync(d.ptr, hin, bp, cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(d.ids, hin + bp, bi, cudaMemcpyHostToDevice);
+        if (bv) cudaMemcpyAsync(d.vals, hin + bp + bi, bv, cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(d.verts, hin + bp + bi + bv, bx, cudaMemcpyHostToDevice);
+        auto fetch = [&](auto& r) {
+            const size_t oi = sizeof(int) * r.nnz, ox = sizeof(float) * 4 * r.nverts;
+            if (!hout) {
+                out_cap = oi + ox;
+                if (cudaMallocHost(&hout, out_cap) != cudaSuccess) return 3;
+            }
+            if (oi + ox > out_cap) return 3;
+            cudaMemcpyAsync(hout, r.ids, oi, cudaMemcpyDeviceToHost);
+            cudaMemcpyAsync(hout + oi, r.verts, ox, cudaMemcpyDeviceToHost);
+            *d2h_bytes = (int64_t)(oi + ox);
+            return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+        };
+        double ms = 0;
+        if (scheme == 1) {
+            CatmullClark::MeshInfo<int, int, int, float> r;
+            rc = call<CatmullClark>(*in, d, levels, r);
+            if (!rc) rc = fetch(r);
+            ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            r.freeAndReset();
+        } else {
+            LAKCatmullClark::MeshInfo<int, int, int, float> r;
+            rc = call<LAKCatmullClark>(*in, d, levels, r);
+            if (!rc) rc = fetch(r);
+            ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            r.freeAndReset();
+        }
+        if (i >= 0) ms_each[i] = ms;
+    }
+    cap.finish();
+    cudaFreeHost(hin);
+    if (hout) cudaFreeHost(hout);
     return rc;
 }
 

@@ -18,7 +18,7 @@ PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING = 1, 2, 4, 8
 
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
-           "slak_subdivide_level_noalloc", "slak_plan_create",
+           "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_destroy", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
@@ -72,6 +72,8 @@ def lib():
         L.slak_last_error_detail.restype = ctypes.c_char_p
         L.slak_subdivide.argtypes = [P, P, I, I, V]
         L.slak_mesh_free.argtypes = [P]
+        L.slak_workspace_release.argtypes = []
+        L.slak_workspace_release.restype = I
         L.slak_subdivide_level_noalloc.argtypes = [P, P, I, V]
         L.slak_plan_create.argtypes = [P, I, I, I, V, ctypes.POINTER(V)]
         L.slak_plan_execute.argtypes = [V, V]

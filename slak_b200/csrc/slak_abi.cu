@@ -130,6 +130,7 @@ struct slak_plan {
     float* ping_verts[2] = {nullptr, nullptr};
     DevStatus* st = nullptr;
     DevStatus* h_st = nullptr;       // pinned
+    bool h_st_owned = true;
     int64_t maxN = 0, maxV = 0, maxE = 0;
     bool any_poly = false;
     int64_t exN = 0, stN = 0, stV = 0, stE = 0, slN = 0, mid_ids = 0, mid_verts = 0;
@@ -373,7 +374,7 @@ void free_plan_memory(slak_plan* p)
     p->gexec = nullptr;
     if (p->arena && p->arena_owned) cudaFree(p->arena);
     p->arena = nullptr;
-    if (p->h_st) cudaFreeHost(p->h_st);
+    if (p->h_st && p->h_st_owned) cudaFreeHost(p->h_st);
     p->h_st = nullptr;
     if (p->out_owned) {
         if (p->out.ids) cudaFree(p->out.ids);
@@ -385,15 +386,25 @@ void free_plan_memory(slak_plan* p)
 }
 
 // Reads level 0's topology once to size the whole plan.
-int probe_level0(slak_plan* p, Level& L0, cudaStream_t str)
+size_t probe_bytes(const Level& L0)
 {
     Carver dry(nullptr);
     Scratch s;
     carve_scratch(dry, s, L0.N, L0.V, 1, !L0.quad);
     dry.take<DevStatus>(1);
-    void* mem = nullptr;
-    cudaError_t e = cudaMalloc(&mem, dry.off);
-    if (e != cudaSuccess) return cuda_status(e);
+    return dry.off;
+}
+
+// `given` (at least probe_bytes) is used when non-null; else the probe allocates.
+int probe_level0(slak_plan* p, Level& L0, cudaStream_t str, void* given = nullptr)
+{
+    Scratch s;
+    void* mem = given;
+    cudaError_t e = cudaSuccess;
+    if (!given) {
+        e = cudaMalloc(&mem, probe_bytes(L0));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
     Carver cv((char*)mem);
     carve_scratch(cv, s, L0.N, L0.V, 1, !L0.quad);
     DevStatus* st = cv.take<DevStatus>(1);
@@ -404,7 +415,7 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str)
     cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
-    cudaFree(mem);
+    if (!given) cudaFree(mem);
     if (lc.err) return lc.err;
     if (e != cudaSuccess) { g_detail = std::string("level-0 probe: ") + cudaGetErrorString(e); return cuda_status(e); }
     if (p->h_st->err) { g_detail = "level-0 probe: device detail " + std::to_string(p->h_st->detail); return p->h_st->err; }
@@ -556,7 +567,109 @@ void plan_wire(slak_plan* p)
     }
 }
 
+// One-shot calls (slak_subdivide) reuse a per-device workspace: the arena of
+// intermediate levels and the pinned status word stay allocated between calls
+// instead of a cudaMalloc / cudaFree pair per call.  A call takes the
+// workspace exclusively (a concurrent call on the same device allocates its
+// own) and returns it only after its stream has synchronized, so the next call
+// on any stream finds it idle.  slak_workspace_release frees it;
+// SLAK_WORKSPACE_CACHE=0 disables the cache.
+struct Workspace {
+    void* mem = nullptr;
+    size_t bytes = 0;
+    DevStatus* h_st = nullptr;
+    bool busy = false;
+};
+constexpr int kWsMaxDevices = 64;
+std::mutex g_ws_mu;
+Workspace g_ws[kWsMaxDevices];
+
+Workspace* workspace_acquire()
+{
+    const char* env = std::getenv("SLAK_WORKSPACE_CACHE");
+    if (env && env[0] == '0') return nullptr;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kWsMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    Workspace* w = &g_ws[dev];
+    if (w->busy) return nullptr;
+    if (!w->h_st && cudaMallocHost(&w->h_st, sizeof(DevStatus)) != cudaSuccess) { w->h_st = nullptr; return nullptr; }
+    w->busy = true;
+    return w;
+}
+
+void workspace_return(Workspace* w)
+{
+    if (!w) return;
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    w->busy = false;
+}
+
+// grows (never shrinks) the workspace to `bytes`
+cudaError_t workspace_reserve(Workspace* w, size_t bytes)
+{
+    if (w->bytes >= bytes) return cudaSuccess;
+    if (w->mem) cudaFree(w->mem);
+    w->mem = nullptr;
+    w->bytes = 0;
+    cudaError_t e = cudaMalloc(&w->mem, bytes);
+    if (e == cudaSuccess) w->bytes = bytes;
+    return e;
+}
+
 }  // namespace
+
+// Plan creation; with `ws`, the arena and the status word come from the
+// workspace (the plan does not own them).
+static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, int flags, cudaStream_t str,
+                            Workspace* ws, slak_plan** out_plan)
+{
+    *out_plan = nullptr;
+    int rc = validate_mesh(cm, scheme);
+    if (rc != SLAK_OK) return rc;
+    slak_plan* p = new (std::nothrow) slak_plan();
+    if (!p) return SLAK_ERR_OOM;
+    const int nlev = plan_init(p, cm, target_level, scheme, flags);
+    cudaError_t ce = cudaSuccess;
+    if (ws) { p->h_st = ws->h_st; p->h_st_owned = false; }
+    else ce = cudaMallocHost(&p->h_st, sizeof(DevStatus));
+    if (ce != cudaSuccess) { p->h_st = nullptr; delete p; return cuda_status(ce); }
+    if (nlev == 0) { *out_plan = p; return SLAK_OK; }
+    void* probe_mem = nullptr;
+    if (ws) {
+        ce = workspace_reserve(ws, probe_bytes(p->lv[0]));
+        if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
+        probe_mem = ws->mem;
+    }
+    rc = probe_level0(p, p->lv[0], str, probe_mem);
+    if (rc == SLAK_OK) rc = plan_levels(p);
+    if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
+    Carver dry(nullptr);
+    plan_carve(p, dry);
+    if (ws) {
+        ce = workspace_reserve(ws, dry.off);
+        p->arena = ws->mem;
+        p->arena_owned = false;
+    } else {
+        ce = cudaMalloc(&p->arena, dry.off);
+    }
+    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
+    Carver cv((char*)p->arena);
+    plan_carve(p, cv);
+    // final outputs (caller-ownable, one allocation each)
+    slak_mesh o = plan_output_shape(p);
+    ce = cudaMalloc(&o.ids, sizeof(int) * (size_t)o.nnz);
+    if (ce == cudaSuccess) ce = cudaMalloc(&o.verts, sizeof(float) * 4 * (size_t)o.nverts);
+    if (ce == cudaSuccess && scheme == SLAK_SCHEME_LAK) {
+        ce = cudaMalloc(&o.ptr, sizeof(int) * (size_t)(o.nfaces + 1));
+        if (ce == cudaSuccess) ce = cudaMalloc(&o.vals, sizeof(int) * (size_t)o.nnz);
+    }
+    p->out = o;
+    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
+    plan_wire(p);
+    *out_plan = p;
+    return SLAK_OK;
+}
 
 extern "C" {
 
@@ -583,38 +696,8 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
                      slak_plan** out_plan)
 {
     if (!cm || !out_plan) return SLAK_ERR_INVALID_ARG;
-    *out_plan = nullptr;
-    int rc = validate_mesh(cm, scheme);
-    if (rc != SLAK_OK) return rc;
-    slak_plan* p = new (std::nothrow) slak_plan();
-    if (!p) return SLAK_ERR_OOM;
-    cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
-    const int nlev = plan_init(p, cm, target_level, scheme, flags);
-    cudaError_t ce = cudaMallocHost(&p->h_st, sizeof(DevStatus));
-    if (ce != cudaSuccess) { delete p; return cuda_status(ce); }
-    if (nlev == 0) { *out_plan = p; return SLAK_OK; }
-    rc = probe_level0(p, p->lv[0], str);
-    if (rc == SLAK_OK) rc = plan_levels(p);
-    if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
-    Carver dry(nullptr);
-    plan_carve(p, dry);
-    ce = cudaMalloc(&p->arena, dry.off);
-    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
-    Carver cv((char*)p->arena);
-    plan_carve(p, cv);
-    // final outputs (caller-ownable, one allocation each)
-    slak_mesh o = plan_output_shape(p);
-    ce = cudaMalloc(&o.ids, sizeof(int) * (size_t)o.nnz);
-    if (ce == cudaSuccess) ce = cudaMalloc(&o.verts, sizeof(float) * 4 * (size_t)o.nverts);
-    if (ce == cudaSuccess && scheme == SLAK_SCHEME_LAK) {
-        ce = cudaMalloc(&o.ptr, sizeof(int) * (size_t)(o.nfaces + 1));
-        if (ce == cudaSuccess) ce = cudaMalloc(&o.vals, sizeof(int) * (size_t)o.nnz);
-    }
-    p->out = o;
-    if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
-    plan_wire(p);
-    *out_plan = p;
-    return SLAK_OK;
+    return plan_create_impl(cm, target_level, scheme, flags, reinterpret_cast<cudaStream_t>(stream), nullptr,
+                            out_plan);
 }
 
 int slak_plan_execute(slak_plan* p, slak_stream_t stream)
@@ -722,8 +805,13 @@ int slak_subdivide(const slak_mesh* cm, slak_mesh* rm, int target_level, int sch
 {
     if (!cm || !rm) return SLAK_ERR_INVALID_ARG;
     slak_plan* p = nullptr;
-    int rc = slak_plan_create(cm, target_level, scheme, 0, stream, &p);
-    if (rc != SLAK_OK) return rc;
+    Workspace* ws = workspace_acquire();
+    int rc = plan_create_impl(cm, target_level, scheme, 0, reinterpret_cast<cudaStream_t>(stream), ws, &p);
+    if (rc != SLAK_OK) { workspace_return(ws); return rc; }
+    struct Return {      // the workspace goes back after the plan's last stream sync
+        Workspace* w;
+        ~Return() { workspace_return(w); }
+    } ret{ws};
     if (p->lv.empty()) { slak_plan_destroy(p); return SLAK_OK; }   // rmesh left untouched
     rc = slak_plan_execute(p, stream);
     if (rc == SLAK_OK) rc = slak_plan_status(p, stream);
@@ -736,6 +824,21 @@ int slak_subdivide(const slak_mesh* cm, slak_mesh* rm, int target_level, int sch
     }
     slak_plan_destroy(p);
     return rc;
+}
+
+int slak_workspace_release(void)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= kWsMaxDevices) return SLAK_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    Workspace* w = &g_ws[dev];
+    if (w->busy) return SLAK_ERR_NOT_READY;
+    if (w->mem) e = cudaFree(w->mem);
+    if (w->h_st) cudaFreeHost(w->h_st);
+    *w = Workspace{};
+    return cuda_status(e);
 }
 
 int slak_mesh_free(slak_mesh* m)
@@ -775,6 +878,7 @@ struct slak_batch {
     std::vector<cudaEvent_t> fork, join;
     cudaGraphExec_t gexec = nullptr;
     DevStatus* h_st = nullptr;                  // pinned, one per mesh
+    DevStatus* d_st = nullptr;                  // device, one per mesh (outlives the waves' arenas)
     int64_t launches = 0;
     int executed = 0;
 };
@@ -793,6 +897,7 @@ void batch_free(slak_batch* b)
     for (auto e : b->join) cudaEventDestroy(e);
     if (b->out_mem) cudaFree(b->out_mem);
     if (b->arena) cudaFree(b->arena);
+    if (b->d_st) cudaFree(b->d_st);
     if (b->h_st) cudaFreeHost(b->h_st);
     delete b;
 }
@@ -930,12 +1035,14 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
         size_t cap = size_t(24) << 30;
         if (const char* wb = std::getenv("SLAK_BATCH_WAVE_BYTES")) cap = (size_t)std::strtoull(wb, nullptr, 10);
         if (budget > cap) budget = cap;
-        // greedy waves in mesh order
+        // greedy waves in mesh order; a mesh above the wave cap (but within
+        // free memory) runs in a wave of its own
+        const size_t hard = rc == SLAK_OK ? (freeb - total_out - margin) * 3 / 4 : 0;
         std::vector<int64_t> cur;
         size_t cur_b = 0;
         for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
             if (!b->plans[i]) continue;
-            if (ab[i] > budget) { g_detail = "mesh " + std::to_string(i) + " needs more scratch than is free"; rc = SLAK_ERR_OOM; break; }
+            if (ab[i] > hard) { g_detail = "mesh " + std::to_string(i) + " needs more scratch than is free"; rc = SLAK_ERR_OOM; break; }
             if (cur_b + ab[i] > budget && !cur.empty()) {
                 b->waves.push_back(cur);
                 b->arena_bytes = std::max(b->arena_bytes, cur_b);
@@ -950,6 +1057,7 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
     if (rc == SLAK_OK && total_out) {
         ce = cudaMalloc(&b->out_mem, total_out);
         if (ce == cudaSuccess && b->arena_bytes) ce = cudaMalloc(&b->arena, b->arena_bytes);
+        if (ce == cudaSuccess) ce = cudaMalloc(&b->d_st, sizeof(DevStatus) * (size_t)count);
         if (ce != cudaSuccess) rc = cuda_status(ce);
     }
     if (rc == SLAK_OK) {
@@ -971,6 +1079,7 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
                 p->arena = static_cast<char*>(b->arena) + off;
                 Carver cv(static_cast<char*>(p->arena));
                 plan_carve(p, cv);
+                p->st = b->d_st + i;           // the arena is reused by later waves
                 off += ab[i];
                 p->out = b->outs[i];
                 plan_wire(p);

@@ -1,0 +1,58 @@
+"""The multi-GPU form is replicas only: every rank refines its own meshes and
+the only collectives are the timing reductions.  These run as two gloo ranks
+on the CPU: max-over-ranks timing, and the partition of the batched workload
+(every mesh on exactly one rank, sizes summing to the whole)."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, ws, port, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    import bench
+    t = bench._max_over_ranks(dist, 1.5 + rank)
+    bench._barrier(dist)
+    sizes = [(it.kind, it.faces, it.levels, it.seed) for it in bench.batch_shard(2000, rank, ws)]
+    q.put((rank, t, sizes))
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_time_and_partition():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    assert [t for _, t, _ in res] == [2.5, 2.5]          # max over ranks, seen by both
+    sys.path.insert(0, ROOT)
+    import bench
+    whole = [(it.kind, it.faces, it.levels, it.seed) for it in bench.batch_shard(2000)]
+    shards = [s for _, _, s in res]
+    assert len(shards[0]) + len(shards[1]) == len(whole)
+    merged = [None] * len(whole)
+    for r, sh in enumerate(shards):
+        for k, item in enumerate(sh):
+            merged[2 * k + r] = item
+    assert merged == whole
