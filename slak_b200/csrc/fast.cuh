@@ -7,11 +7,11 @@
 // general path rebuilds with atomics, sorting and searching is then known in
 // closed form from P's adjacency state:
 //
-//   sptr1 / sc1   P's vertex columns (corners of each vertex, corner order)
-//   slot1         inverse of sc1 (corner -> its slot)
+//   sptr1         P's vertex columns (offsets; a column holds its vertex's
+//                 corners in corner order)
+//   slot1         corner -> its slot in its vertex's column
 //   tw1           twin half-edge of each corner of P
 //   t1            slot1[tw1[prev(x)]] (SLAK)
-//   H1            P's edges in the scheme's numbering: (min->max, max->min)
 //
 // C's adjacency: vertex v < V1 keeps its column with corners 4x (x in
 // column order), face point V1+g owns corners 4x+2 of g's four corners,
@@ -26,7 +26,8 @@
 //   k_g1  per quad of C (4 threads per face of P): C's refined quads, face
 //         points of C, vertex points of the face points of P, SLAK edge points
 //         N1+x, and the next level's per-corner state
-//   k_g2  per edge of P: vertex points of the edge points of P, LAK edge points
+//   k_g2  per edge of P, visited in corner order (the min->max half-edge's
+//         lane): vertex points of the edge points of P, LAK edge points
 //   k_g3  per vertex of P: vertex points of P's vertices and SLAK edge points
 //         slot1(x), streamed from slot-ordered records k_g1 scatters
 // The float arithmetic and its order are exactly the general path's (and the
@@ -43,11 +44,9 @@ __device__ __forceinline__ int qprev(int x) { return (x & ~3) | ((x + 3) & 3); }
 // P's adjacency state (read) / C's (written when another level follows)
 struct QState {
     int* sptr;
-    int* sc;
     int* slot;
     int* tw;
     int* t;
-    int2* H;
 };
 
 struct FastDims {
@@ -217,44 +216,51 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
         reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
         reinterpret_cast<int4*>(c.slot)[x] =
             make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
-        c.sc[s1] = 4 * x;                                          // old vertex column, slot s1
-        if (!LAK) {
-            c.H[s1] = make_int2(4 * x, 4 * ntw + 3);               // SLAK edge slot1(x)
+        if (!LAK)
             reinterpret_cast<int4*>(c.t)[x] =
                 make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
-            c.H[d.N1 + x] = make_int2(4 * x + 2, 4 * px + 1);     // SLAK edge N1 + x
-        }
-        c.sc[d.N1 + x] = 4 * x + 2;                                // face point column
         if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// G2: one thread per edge e of P, half-edges (h, h2) = H1[e] (min->max, max->min of P)
+// G2: the edges of P, visited in corner order.  Thread x is corner x of P (=
+// quad x of C); the 4 corners of a face of P are 4 consecutive lanes.  Edge e
+// of P with half-edges (h, h2) = (min->max, max->min) is computed by the lane
+// x = h, so the quantities of h's face (v, u, P's face point, C's face points
+// of quads h and next(h)) are coalesced loads or shuffles, and only the twin
+// face's three (its face point, C's face points of quads h2 and next(h2)) are
+// gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
 template <bool LAK, bool STATE>
 __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
                                                QState p, QState c, float* __restrict__ R)
 {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= d.E1) return;
-    const int2 hh = __ldg(p.H + e);
-    const int h = hh.x, h2 = hh.y, nh = qnext(h), nh2 = qnext(h2);
-    const int ve = d.V1 + d.F1 + e;
-    const int v = __ldg(ids + 4 * h), u = __ldg(ids + 4 * h2);
-    const int fh = d.V1 + (h >> 2), fh2 = d.V1 + (h2 >> 2);
-    const float4 Pv = ldg4(P, v), Pu = ldg4(P, u), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2), Pe = ldg4(P, ve);
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = x < d.N1;
+    const int lane = threadIdx.x & 31, q = x & 3;
+    const int ln = (lane & ~3) | ((q + 1) & 3);
     const float* FP = R + 4 * (int64_t)d.V;
-    const float4 Fh = ldg4(FP, h), Fh2 = ldg4(FP, h2), Fnh = ldg4(FP, nh), Fnh2 = ldg4(FP, nh2);
+    // two dependent rounds of loads: the coalesced ones, then every gather at once
+    const int4 Q = valid ? __ldg(reinterpret_cast<const int4*>(ids) + x) : make_int4(0, 0, 0, 0);
+    const int h2 = valid ? __ldg(p.tw + x) : 0;
+    const float4 Fh = valid ? ldg4(FP, x) : f4_zero();
+    const int u = __shfl_sync(0xffffffffu, Q.x, ln);
+    const float4 Fnh = shfl4(Fh, ln);
+    if (!valid || Q.x >= u) return;              // not the min->max half-edge of its edge
+    const int h = x, nh = qnext(h), nh2 = qnext(h2);
+    const int ve = Q.y, e = Q.y - d.V1 - d.F1;
+    const int fh = Q.z, fh2 = d.V1 + (h2 >> 2);
+    const float4 Pv = ldg4(P, Q.x), Pu = ldg4(P, u);
+    const float4 Pe = ldg4(P, ve), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2);
+    const float4 Fh2 = ldg4(FP, h2), Fnh2 = ldg4(FP, nh2);
     // corners of the edge point: A=4h+1 (nbr fh, face h), B=4h2+1 (fh2, h2), C=4nh+3 (u, nh), D=4nh2+3 (v, nh2)
     const int A = 4 * h + 1, B = 4 * h2 + 1, Cc = 4 * nh + 3, D = 4 * nh2 + 3;
-    const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D), rD = rank4(D, A, B, Cc);
+    const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D);
     float4 nb[4], fq[4];
-    int co[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         nb[r] = rA == r ? Pf : rB == r ? Pf2 : rC == r ? Pu : Pv;
         fq[r] = rA == r ? Fh : rB == r ? Fh2 : rC == r ? Fnh : Fnh2;
-        co[r] = rA == r ? A : rB == r ? B : rC == r ? Cc : D;
     }
     float4 yv;
     if (!LAK) {
@@ -268,10 +274,10 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict
         float4 acc = f4_zero();
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc = f4_add(acc, fq[r]);
-        // tails {v, u, fh, fh2} in ascending id: v,u < V1 <= fh, fh2
-        const bool vu = v < u, ff = fh < fh2;
-        acc = f4_add(acc, vu ? Pv : Pu);
-        acc = f4_add(acc, vu ? Pu : Pv);
+        // tails {v, u, fh, fh2} in ascending id: v < u < V1 <= fh, fh2
+        const bool ff = fh < fh2;
+        acc = f4_add(acc, Pv);
+        acc = f4_add(acc, Pu);
         acc = f4_add(acc, ff ? Pf : Pf2);
         acc = f4_add(acc, ff ? Pf2 : Pf);
         yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(Pe, 2.0f)), 4.0f);
@@ -279,31 +285,19 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict
     st4_cs(R, ve, yv);
 
     if (LAK) {
-        // edges 4e + {lower end, higher end, lower face point, higher face point}
+        // edges 4e + {lower end, higher end, lower face point, higher face point}; v < u
         const float4 Ev = f4_mul(f4_add(f4_add(f4_add(Pv, Pe), Fh), Fnh2), 0.25f);
         const float4 Eu = f4_mul(f4_add(f4_add(f4_add(Pu, Pe), Fh2), Fnh), 0.25f);
         const float4 Ef = f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f);
         const float4 Ef2 = f4_mul(f4_add(f4_add(f4_add(Pf2, Pe), Fnh2), Fh2), 0.25f);
-        const bool vu = v < u, ff = fh < fh2;
+        const bool ff = fh < fh2;
         const int64_t base = (int64_t)d.V + d.N1 + 4 * (int64_t)e;
-        st4_cs(R, base + 0, vu ? Ev : Eu);
-        st4_cs(R, base + 1, vu ? Eu : Ev);
+        st4_cs(R, base + 0, Ev);
+        st4_cs(R, base + 1, Eu);
         st4_cs(R, base + 2, ff ? Ef : Ef2);
         st4_cs(R, base + 3, ff ? Ef2 : Ef);
-        if (STATE) {
-            const int2 Hv = make_int2(4 * h, 4 * nh2 + 3), Hu = make_int2(4 * h2, 4 * nh + 3);
-            const int2 Hf = make_int2(4 * nh + 2, 4 * h + 1), Hf2 = make_int2(4 * nh2 + 2, 4 * h2 + 1);
-            int2* H = c.H + 4 * (int64_t)e;
-            H[0] = vu ? Hv : Hu;
-            H[1] = vu ? Hu : Hv;
-            H[2] = ff ? Hf : Hf2;
-            H[3] = ff ? Hf2 : Hf;
-        }
     }
-    if (STATE) {
-        reinterpret_cast<int4*>(c.sc + 2 * (int64_t)d.N1)[e] = make_int4(co[0], co[1], co[2], co[3]);
-        c.sptr[ve] = 2 * d.N1 + 4 * e;
-    }
+    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -324,6 +318,57 @@ __global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const float* __restri
     const float nn = (float)(n * n);
     const float4* Z = z.Z;
     float4 yv;
+    if (n <= 4) {
+        // the common case: every record of the column loaded up front (the
+        // arithmetic and its order are the loops' below)
+        float4 zf[4], zn[4], bb[4];
+        int tt[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < n) {
+                zf[k] = __ldg(Z + 2 * (int64_t)(b + k));
+                zn[k] = __ldg(Z + 2 * (int64_t)(b + k) + 1);
+                if (!LAK) bb[k] = __ldg(z.B + b + k);
+                else tt[k] = __ldg(z.T + b + k);
+            }
+        }
+        float4 acc = f4_zero();
+        if (!LAK) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n) acc = f4_add(acc, zn[k]);
+            yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n) yv = f4_add(yv, f4_div(zf[k], nn));
+            const int64_t EPb = (int64_t)d.V + d.N1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n)
+                    st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), f4_mul(f4_add(Pv, zf[k]), 0.25f)), bb[k]));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n) acc = f4_add(acc, zf[k]);
+            // the tails in ascending id (ids in a column are distinct)
+            int rk[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                rk[k] = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) rk[k] += (j < n && tt[j] < tt[k]);
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (k < n && rk[k] == r) acc = f4_add(acc, zn[k]);
+            yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
+        }
+        st4(R, v, yv);
+        if (STATE) c.sptr[v] = b;
+        return;
+    }
     const bool comp = compensated && n > 4;
     if (!LAK) {
         if (!comp) {

@@ -46,30 +46,49 @@ __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __rest
     atomicAdd(cnt + v, 1);
 }
 
-// slot order from the atomic is arbitrary; k_vsort makes it canonical
+// slot order from the atomic is arbitrary (the unsorted column goes to
+// `loose`); k_vsort makes it canonical
 __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
-                         int* __restrict__ fill, int* __restrict__ sc)
+                         int* __restrict__ fill, int* __restrict__ loose)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     int v = ids[c];
     if ((unsigned)v >= (unsigned)V) return;
     int r = atomicSub(fill + v, 1) - 1;
-    sc[sptr[v] + r] = c;
+    loose[sptr[v] + r] = c;
 }
 
+// Each column sorted by corner index: a corner's slot is the number of smaller
+// corners in its column (corner indices are distinct).  Columns of up to 8 are
+// ranked in registers; longer ones (high-valence vertices) read the unsorted
+// column n times, with independent loads rather than a chain of dependent ones.
 template <bool QUAD>
 __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
-                        int* __restrict__ sc, int* __restrict__ snext, int* __restrict__ sprev,
-                        int* __restrict__ sprevc)
+                        const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
+                        int* __restrict__ sprev, int* __restrict__ sprevc)
 {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
-    const int b = sptr[v], e = sptr[v + 1];
-    for (int i = b + 1; i < e; ++i) {      // insertion sort: columns are short
-        int x = sc[i], j = i - 1;
-        while (j >= b && sc[j] > x) { sc[j + 1] = sc[j]; --j; }
-        sc[j + 1] = x;
+    const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    if (n <= 8) {
+        int u[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u[k] = k < n ? __ldg(loose + b + k) : INT32_MAX;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            int r = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) r += u[j] < u[k];
+            if (k < n) sc[b + r] = u[k];
+        }
+    } else {
+        for (int i = b; i < e; ++i) {
+            const int x = __ldg(loose + i);
+            int r = 0;
+            for (int j = b; j < e; ++j) r += __ldg(loose + j) < x;
+            sc[b + r] = x;
+        }
     }
     for (int s = b; s < e; ++s) {
         int c = sc[s];
@@ -85,47 +104,116 @@ __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, cons
 // SLAK owner: the half-edge min->max, or the only half-edge of a boundary edge
 // (epids_tmp = v0 < v1, set to 1 by checkForBoundary*, CatmullClarkKernels.cuh:159,235).
 // LAK edges of column v are its distinct neighbours u < v (createEVals, spgemm.cuh:71-100).
+//
+// One slot's result, given the column as (next vertex, previous vertex,
+// previous corner) per slot; NMAX > 0 unrolls over a column held in registers.
+template <bool LAK, int NMAX, class Col>
+__device__ __forceinline__ void edge_slot(const Col& col, int n, int k, int v, int& tw, int& fl, int& own,
+                                          int& bad)
+{
+    const int w = col.nx(k), u = col.pv(k);
+    int in_twin = 0;
+    tw = -1;
+    bool dn = w < v, dp = u < v && u != w;
+#pragma unroll
+    for (int t = 0; t < (NMAX > 0 ? NMAX : n); ++t) {
+        if (NMAX > 0 && t >= n) break;
+        const int nt = col.nx(t), pt = col.pv(t);
+        if (pt == w) { if (tw < 0) tw = col.pc(t); else bad = 1; }
+        if (nt == u) in_twin = 1;
+        if (t < k) {
+            if (nt == w) bad = 1;
+            if (LAK) {
+                if (nt == w || pt == w) dn = false;
+                if (nt == u || pt == u) dp = false;
+            }
+        }
+    }
+    if (w == v || u == v) bad = 1;
+    fl = (tw < 0 ? SF_BOUT : 0) | (in_twin ? 0 : SF_BIN);
+    own = 0;
+    if (!LAK) {
+        if (v < w || tw < 0) { fl |= SF_OWNER; own = 1; }
+    } else {
+        own = (int)dn + (int)dp;            // enumerated as snext[0], sprev[0], snext[1], ...
+    }
+}
+
+struct ColGlobal {       // column slots b.. in global memory
+    const int *snext, *sprev, *sprevc;
+    int b;
+    __device__ int nx(int t) const { return __ldg(snext + b + t); }
+    __device__ int pv(int t) const { return __ldg(sprev + b + t); }
+    __device__ int pc(int t) const { return __ldg(sprevc + b + t); }
+};
+struct ColRegs {         // a column of at most 8 slots in registers
+    int n_[8], p_[8], c_[8];
+    __device__ int nx(int t) const { return n_[t]; }
+    __device__ int pv(int t) const { return p_[t]; }
+    __device__ int pc(int t) const { return c_[t]; }
+};
+
+// Columns of up to 8 slots are handled by their own thread from registers; a
+// longer column (a high-valence vertex) is shared by its warp's 32 lanes, one
+// slot per lane, so no thread walks n^2 pairs alone.
 template <bool LAK>
 __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ snext,
                         const int* __restrict__ sprev, const int* __restrict__ sprevc, int* __restrict__ stw,
                         int* __restrict__ sflag, int* __restrict__ ecnt, int* __restrict__ bcount, DevStatus* st)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    int nb = 0;
-    if (v < V) {
-        const int b = sptr[v], e = sptr[v + 1];
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int nb = 0, b = 0, n = 0;
+    if (v < V) { b = sptr[v]; n = sptr[v + 1] - b; }
+    if (v < V && n <= 8) {
+        ColRegs col;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            col.n_[k] = k < n ? __ldg(snext + b + k) : -1;
+            col.p_[k] = k < n ? __ldg(sprev + b + k) : -1;
+            col.c_[k] = k < n ? __ldg(sprevc + b + k) : -1;
+        }
         int own = 0, bad = 0;
-        for (int s = b; s < e; ++s) {
-            const int w = snext[s], u = sprev[s];
-            int tw = -1, in_twin = 0;
-            for (int t = b; t < e; ++t) {
-                if (sprev[t] == w) { if (tw < 0) tw = sprevc[t]; else bad = 1; }
-                if (snext[t] == u) in_twin = 1;
-                if (t < s && snext[t] == w) bad = 1;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < n) {
+                int tw, fl, o;
+                edge_slot<LAK, 8>(col, n, k, v, tw, fl, o, bad);
+                own += o;
+                nb += tw < 0;
+                stw[b + k] = tw;
+                sflag[b + k] = fl;
             }
-            if (w == v || u == v) bad = 1;
-            int fl = (tw < 0 ? SF_BOUT : 0) | (in_twin ? 0 : SF_BIN);
-            if (!LAK) {
-                if (v < w || tw < 0) { fl |= SF_OWNER; ++own; }
-            } else {
-                // distinct smaller neighbours, enumerated as snext[b], sprev[b], snext[b+1], ...
-                bool dn = w < v, dp = u < v && u != w;
-                for (int t = b; t < s; ++t) {
-                    if (snext[t] == w || sprev[t] == w) dn = false;
-                    if (snext[t] == u || sprev[t] == u) dp = false;
-                }
-                own += (int)dn + (int)dp;
-            }
-            nb += tw < 0;
-            stw[s] = tw;
-            sflag[s] = fl;
         }
         ecnt[v] = own;
         if (bad) set_error(st, 4, v);
     }
+    unsigned big = __ballot_sync(0xffffffffu, v < V && n > 8);
+    while (big) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int bv = __shfl_sync(0xffffffffu, v, src), bb = __shfl_sync(0xffffffffu, b, src);
+        const int bn = __shfl_sync(0xffffffffu, n, src);
+        const ColGlobal col{snext, sprev, sprevc, bb};
+        int own = 0, bad = 0;
+        for (int k = lane; k < bn; k += 32) {
+            int tw, fl, o;
+            edge_slot<LAK, 0>(col, bn, k, bv, tw, fl, o, bad);
+            own += o;
+            nb += tw < 0;
+            stw[bb + k] = tw;
+            sflag[bb + k] = fl;
+        }
+        for (int o = 16; o > 0; o >>= 1) own += __shfl_down_sync(0xffffffffu, own, o);
+        bad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) {
+            ecnt[bv] = own;
+            if (bad) set_error(st, 4, bv);
+        }
+    }
     // boundary half-edge count of the level
     for (int o = 16; o > 0; o >>= 1) nb += __shfl_down_sync(0xffffffffu, nb, o);
-    if ((threadIdx.x & 31) == 0 && nb) atomicAdd(bcount, nb);
+    if (lane == 0 && nb) atomicAdd(bcount, nb);
 }
 
 // SLAK edge ids: owners in slot order get eptr[v] + rank; the twin shares it.

@@ -133,7 +133,7 @@ struct slak_plan {
     bool h_st_owned = true;
     int64_t maxN = 0, maxV = 0, maxE = 0;
     bool any_poly = false;
-    int64_t exN = 0, stN = 0, stV = 0, stE = 0, slN = 0, mid_ids = 0, mid_verts = 0;
+    int64_t exN = 0, stN = 0, stV = 0, slN = 0, mid_ids = 0, mid_verts = 0;
     bool arena_owned = true;
     QState qs[2]{};
     SlotScratch slots{};
@@ -176,14 +176,12 @@ void carve_export(Carver& cv, Scratch& s, int64_t N)
     s.xt = cv.take<int>(N);
 }
 
-void carve_state(Carver& cv, QState& q, int64_t N, int64_t V, int64_t E)
+void carve_state(Carver& cv, QState& q, int64_t N, int64_t V)
 {
     q.sptr = cv.take<int>(V + 1);
-    q.sc = cv.take<int>(N);
     q.slot = cv.take<int>(N);
     q.tw = cv.take<int>(N);
     q.t = cv.take<int>(N);
-    q.H = cv.take<int2>(E);
 }
 
 // Topology of a level up to the edge-offset scan (needs no output buffers).
@@ -202,15 +200,18 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     int64_t dummy = 0;
     scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, &dummy);
     lc.after("scan(valence)", 3);
-    k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sc);
+    // the unsorted columns live in sflag until k_edges writes the flags
+    k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sflag);
     lc.after("k_bucket");
     int* bcount = &st->bcount[li];
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
-        k_vsort<true><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc);
+        k_vsort<true><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+                                                       s.sprevc);
     } else {
         Faces<false> fc{L.ptr, s.cface};
-        k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc);
+        k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+                                                        s.sprevc);
     }
     lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
@@ -297,7 +298,7 @@ void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
     k_g1<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
                                                          reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots);
     lc.after("k_g1", 1, g1b);
-    k_g2<LAK, STATE><<<grid_for(Pl.E), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+    k_g2<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
     lc.after("k_g2", 1, g2b);
     k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
                                                              L.o_verts, comp ? 1 : 0);
@@ -495,7 +496,6 @@ int plan_levels(slak_plan* p)
             L.make_state = true;
             if (L.N > p->stN) p->stN = L.N;
             if (L.V > p->stV) p->stV = L.V;
-            if (L.E > p->stE) p->stE = L.E;
         }
     }
     for (int i = 0; i + 1 < nlev; ++i) {
@@ -512,7 +512,7 @@ void plan_carve(slak_plan* p, Carver& cv)
     const int nlev = (int)p->lv.size();
     carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
     if (p->exN) carve_export(cv, p->s, p->exN);
-    if (p->stN) { carve_state(cv, p->qs[0], p->stN, p->stV, p->stE); carve_state(cv, p->qs[1], p->stN, p->stV, p->stE); }
+    if (p->stN) { carve_state(cv, p->qs[0], p->stN, p->stV); carve_state(cv, p->qs[1], p->stN, p->stV); }
     if (p->slN) {
         p->slots.Z = cv.take<float4>(2 * p->slN);
         p->slots.B = cv.take<float4>(p->slN);
@@ -560,7 +560,7 @@ void plan_wire(slak_plan* p)
         Level& L = p->lv[i];
         if (!L.fast) continue;
         const Level& P = p->lv[i - 1];
-        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.sc, p->s.xslot, p->s.xtw, p->s.xt, p->s.H};
+        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.xslot, p->s.xtw, p->s.xt};
         else L.in_state = P.out_state;
         if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
         L.slots = p->slots;
