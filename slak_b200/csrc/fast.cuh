@@ -415,19 +415,7 @@ __global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const float* __restri
 }
 
 // ---------------------------------------------------------------------------------------------
-// State of a quad level built by the general path: corner -> slot, corner -> twin, t (SLAK)
-__global__ void k_export_state(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                               const int* __restrict__ stw, int* __restrict__ slot, int* __restrict__ tw)
-{
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    for (int s = sptr[v]; s < sptr[v + 1]; ++s) {
-        int c = sc[s];
-        slot[c] = s;
-        tw[c] = stw[s];
-    }
-}
-
+// t of a general quad level feeding the fast path (SLAK): t[x] = slot[tw[prev x]]
 __global__ void k_export_t(int N, const int* __restrict__ slot, const int* __restrict__ tw, int* __restrict__ t)
 {
     int x = blockIdx.x * blockDim.x + threadIdx.x;

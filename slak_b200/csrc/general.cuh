@@ -61,17 +61,30 @@ __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* _
 
 // Each column sorted by corner index: a corner's slot is the number of smaller
 // corners in its column (corner indices are distinct).  Columns of up to 8 are
-// ranked in registers; longer ones (high-valence vertices) read the unsorted
-// column n times, with independent loads rather than a chain of dependent ones.
+// ranked by their own thread in registers; a longer column (a high-valence
+// vertex) is ranked by its warp, one corner per lane.  With `xslot` the slot of
+// every corner is exported as well (corner -> slot, for the fast path).
+template <bool QUAD>
+__device__ __forceinline__ void vsort_neighbours(Faces<QUAD> fc, const int* __restrict__ ids, int s, int c,
+                                                 int* __restrict__ snext, int* __restrict__ sprev,
+                                                 int* __restrict__ sprevc)
+{
+    const int p = fc.prev(c);
+    snext[s] = __ldg(ids + fc.next(c));
+    sprev[s] = __ldg(ids + p);
+    sprevc[s] = p;
+}
+
 template <bool QUAD>
 __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
                         const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
-                        int* __restrict__ sprev, int* __restrict__ sprevc)
+                        int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int b = sptr[v], e = sptr[v + 1], n = e - b;
-    if (n <= 8) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int b = 0, n = 0;
+    if (v < V) { b = sptr[v]; n = sptr[v + 1] - b; }
+    if (v < V && n <= 8) {
         int u[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) u[k] = k < n ? __ldg(loose + b + k) : INT32_MAX;
@@ -80,22 +93,26 @@ __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, cons
             int r = 0;
 #pragma unroll
             for (int j = 0; j < 8; ++j) r += u[j] < u[k];
-            if (k < n) sc[b + r] = u[k];
-        }
-    } else {
-        for (int i = b; i < e; ++i) {
-            const int x = __ldg(loose + i);
-            int r = 0;
-            for (int j = b; j < e; ++j) r += __ldg(loose + j) < x;
-            sc[b + r] = x;
+            if (k < n) {
+                sc[b + r] = u[k];
+                if (xslot) xslot[u[k]] = b + r;
+                vsort_neighbours(fc, ids, b + r, u[k], snext, sprev, sprevc);
+            }
         }
     }
-    for (int s = b; s < e; ++s) {
-        int c = sc[s];
-        int p = fc.prev(c);
-        snext[s] = __ldg(ids + fc.next(c));
-        sprev[s] = __ldg(ids + p);
-        sprevc[s] = p;
+    unsigned big = __ballot_sync(0xffffffffu, v < V && n > 8);
+    while (big) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int bb = __shfl_sync(0xffffffffu, b, src), bn = __shfl_sync(0xffffffffu, n, src);
+        for (int k = lane; k < bn; k += 32) {
+            const int x = __ldg(loose + bb + k);
+            int r = 0;
+            for (int j = 0; j < bn; ++j) r += __ldg(loose + bb + j) < x;
+            sc[bb + r] = x;
+            if (xslot) xslot[x] = bb + r;
+            vsort_neighbours(fc, ids, bb + r, x, snext, sprev, sprevc);
+        }
     }
 }
 
@@ -156,10 +173,12 @@ struct ColRegs {         // a column of at most 8 slots in registers
 // Columns of up to 8 slots are handled by their own thread from registers; a
 // longer column (a high-valence vertex) is shared by its warp's 32 lanes, one
 // slot per lane, so no thread walks n^2 pairs alone.
+// With `xtw` the twin of every corner is exported as well (corner -> twin).
 template <bool LAK>
-__global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ snext,
-                        const int* __restrict__ sprev, const int* __restrict__ sprevc, int* __restrict__ stw,
-                        int* __restrict__ sflag, int* __restrict__ ecnt, int* __restrict__ bcount, DevStatus* st)
+__global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                        const int* __restrict__ snext, const int* __restrict__ sprev,
+                        const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
+                        int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -183,6 +202,7 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
                 nb += tw < 0;
                 stw[b + k] = tw;
                 sflag[b + k] = fl;
+                if (xtw) xtw[__ldg(sc + b + k)] = tw;
             }
         }
         ecnt[v] = own;
@@ -203,6 +223,7 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
             nb += tw < 0;
             stw[bb + k] = tw;
             sflag[bb + k] = fl;
+            if (xtw) xtw[__ldg(sc + bb + k)] = tw;
         }
         for (int o = 16; o > 0; o >>= 1) own += __shfl_down_sync(0xffffffffu, own, o);
         bad = __any_sync(0xffffffffu, bad);

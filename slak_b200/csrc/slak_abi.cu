@@ -204,22 +204,25 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sflag);
     lc.after("k_bucket");
     int* bcount = &st->bcount[li];
+    // a general quad level feeding the fast path exports corner -> slot / twin
+    int* xslot = L.export_state ? s.xslot : nullptr;
+    int* xtw = L.export_state ? s.xtw : nullptr;
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
         k_vsort<true><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
-                                                       s.sprevc);
+                                                       s.sprevc, xslot);
     } else {
         Faces<false> fc{L.ptr, s.cface};
         k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
-                                                        s.sprevc);
+                                                        s.sprevc, xslot);
     }
     lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
-        k_edges<true><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
-                                                        s.ecnt, bcount, st);
+        k_edges<true><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+                                                        s.sflag, s.ecnt, bcount, xtw, st);
     else
-        k_edges<false><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.snext, s.sprev, s.sprevc, s.stw, s.sflag,
-                                                         s.ecnt, bcount, st);
+        k_edges<false><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+                                                         s.sflag, s.ecnt, bcount, xtw, st);
     lc.after("k_edges");
     scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, &dummy);
     lc.after("scan(edges)", 3);
@@ -350,14 +353,9 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         lc.after("k_check_level");
         if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, lc);
         else launch_rest<false>(L, p->scheme, comp, p->s, p->st, lc);
-        if (L.export_state) {
-            k_export_state<<<grid_for(L.V), kBlock, 0, str>>>((int)L.V, p->s.sptr, p->s.sc, p->s.stw, p->s.xslot,
-                                                              p->s.xtw);
-            lc.after("k_export_state");
-            if (p->scheme == SLAK_SCHEME_SLAK) {
-                k_export_t<<<grid_for(L.N), kBlock, 0, str>>>((int)L.N, p->s.xslot, p->s.xtw, p->s.xt);
-                lc.after("k_export_t");
-            }
+        if (L.export_state && p->scheme == SLAK_SCHEME_SLAK) {   // slot / twin came from k_vsort / k_edges
+            k_export_t<<<grid_for(L.N), kBlock, 0, str>>>((int)L.N, p->s.xslot, p->s.xtw, p->s.xt);
+            lc.after("k_export_t");
         }
     }
     p->launches = nl;
