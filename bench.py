@@ -190,6 +190,17 @@ def run_ours(args, dist, rank, ws):
         kern["traffic_note"] = (f"{tpu} B per quad refined (ncu, mixed:384 capture) x {units} quads; "
                                 f"{tpu * units / kern['algorithmic_bytes_per_launch']:.2f}x the algorithmic bytes")
 
+    # ms per level: the per-kernel event times summed by level, with the level's
+    # compulsory bytes against the measured peak
+    peak, _ = _peaks()
+    per_level = []
+    for lv in range(levels):
+        ms_l = sum(t["ms"] for t in ktable if t["level"] == lv)
+        b = stats[lv]["algorithmic_bytes"]
+        per_level.append({"level": lv, "out_faces": stats[lv]["out_faces"], "ms": ms_l, "algorithmic_bytes": b,
+                          "GB/s": b / (ms_l * 1e-3) / 1e9 if ms_l > 0 else None,
+                          "frac": (b / (ms_l * 1e-3) / 1e9) / peak if ms_l > 0 else None})
+
     # e2e: host buffers, the C-ABI drop-in call
     e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws)
 
@@ -206,6 +217,7 @@ def run_ours(args, dist, rank, ws):
         "gpu_launches": launches,
         "roofline": kern,
         "kernels": ktable[:8],
+        "levels": per_level,
         "pipeline_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                               "frac": achieved / peak, "peak_kind": peak_kind,
                               "algorithmic_bytes": alg_bytes},

@@ -85,10 +85,32 @@ struct SlotScratch {
     int* T;
 };
 
-template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
-                                               QState p, QState c, int4* __restrict__ out_ids,
-                                               float* __restrict__ R, SlotScratch z)
+// C's slot / twin / t for its corners 4x+k (the state the next fast level reads)
+template <bool LAK>
+__device__ __forceinline__ void write_state(const FastDims& d, QState& c, int x, int nxx, int px, int tw1x,
+                                            int tw1_px, int ntw, int ntwp, int s1, int t1x, int eidp_x,
+                                            int eidp_px)
+{
+    // edge of P through x: corners A=4x+1, B=4tw1x+1, Cc=4nxx+3, D=4ntw+3
+    const int A = 4 * x + 1, B = 4 * tw1x + 1, Cc = 4 * nxx + 3, D = 4 * ntw + 3;
+    // edge of P through prev(x): A'=4px+1, B'=4tw1_px+1, C'=4x+3, D'=4ntwp+3
+    const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
+    const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
+    reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
+    reinterpret_cast<int4*>(c.slot)[x] =
+        make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
+    if (!LAK)
+        reinterpret_cast<int4*>(c.t)[x] =
+            make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
+}
+
+// P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
+// exchanged by shuffles) or polygons (face offsets and the corner -> face map
+// of P, `pf`; a face's corners are consecutive threads, read from memory).
+template <bool LAK, bool STATE, bool PQ>
+__global__ void __launch_bounds__(kBlock) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                               const float* __restrict__ P, QState p, QState c,
+                                               int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
     __shared__ int4 sq[4 * kBlock];
     const int x0 = blockIdx.x * blockDim.x;
@@ -109,7 +131,18 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
     if (valid) s1 = __ldg(p.slot + x);
     if (valid && !LAK) t1x = __ldg(p.t + x);
     const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
-    const int tw1_px = __shfl_sync(0xffffffffu, tw1x, lp);
+    // next / previous corner of x in its face of P, and the twin of the previous one
+    int nxx, px, tw1_px;
+    if (PQ) {
+        nxx = qnext(x); px = qprev(x);
+        tw1_px = __shfl_sync(0xffffffffu, tw1x, lp);
+    } else {
+        const int f = Q.z - d.V1;              // C's quad x holds P's face point V1 + face(x)
+        const int fb = valid ? __ldg(pf.ptr + f) : 0, fe = valid ? __ldg(pf.ptr + f + 1) : 1;
+        nxx = x + 1 == fe ? fb : x + 1;
+        px = x == fb ? fe - 1 : x - 1;
+        tw1_px = valid && (LAK || STATE) ? __ldg(p.tw + px) : 0;
+    }
     const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
 
     // face point of quad x
@@ -123,13 +156,22 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
     // edge ids of C's corners 4x+k
     int e0, e1, e2, e3;
     if (!LAK) {
-        e0 = s1; e1 = d.N1 + qnext(x); e2 = d.N1 + x; e3 = t1x;
+        e0 = s1; e1 = d.N1 + nxx; e2 = d.N1 + x; e3 = t1x;
     } else {
-        const int vnx = __shfl_sync(0xffffffffu, Q.x, ln), vpx = __shfl_sync(0xffffffffu, Q.x, lp);
-        const int fx = x >> 2;
+        int vnx, vpx, fx, ftw, ftwp;
+        if (PQ) {
+            vnx = __shfl_sync(0xffffffffu, Q.x, ln); vpx = __shfl_sync(0xffffffffu, Q.x, lp);
+            fx = x >> 2; ftw = tw1x >> 2; ftwp = tw1_px >> 2;
+        } else {
+            vnx = valid ? __ldg(ids + 4 * (int64_t)nxx) : 0;
+            vpx = valid ? __ldg(ids + 4 * (int64_t)px) : 0;
+            fx = Q.z - d.V1;
+            ftw = valid ? pf.face(tw1x) : 0;
+            ftwp = valid ? pf.face(tw1_px) : 0;
+        }
         e0 = 4 * eidp_x + (Q.x > vnx);
-        e1 = 4 * eidp_x + 2 + (fx > (tw1x >> 2));
-        e2 = 4 * eidp_px + 2 + (fx > (tw1_px >> 2));
+        e1 = 4 * eidp_x + 2 + (fx > ftw);
+        e2 = 4 * eidp_px + 2 + (fx > ftwp);
         e3 = 4 * eidp_px + (Q.x > vpx);
     }
     // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}: staged, then one coalesced run
@@ -157,70 +199,113 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
         else z.B[t1x] = f4_mul(f4_add(c3, fp), 0.25f);
     }
 
-    // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
-    float4 nb[4], fq[4];
-    int tl[4];
+    if constexpr (!PQ) {
+        // polygon P: P's face points and C's inner edge points are k_gf's
+        if (STATE && valid) {
+            const int ntw = pf.next(tw1x), ntwp = pf.next(tw1_px);
+            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, ntw, ntwp, s1, t1x, eidp_x, eidp_px);
+        }
+    } else {
+        // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
+        float4 nb[4], fq[4];
+        int tl[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        nb[j] = shfl4(LAK ? c1 : c3, gl | j);      // SLAK: e_in(x_j); LAK: tails e_out(x_j)
-        fq[j] = shfl4(fp, gl | j);
-        tl[j] = __shfl_sync(0xffffffffu, Q.y, gl | j);
-    }
-    if (valid && q == 0) {
-        float4 yv;
-        if (!LAK) {
-            float4 acc = f4_zero();
+        for (int j = 0; j < 4; ++j) {
+            nb[j] = shfl4(LAK ? c1 : c3, gl | j);      // SLAK: e_in(x_j); LAK: tails e_out(x_j)
+            fq[j] = shfl4(fp, gl | j);
+            tl[j] = __shfl_sync(0xffffffffu, Q.y, gl | j);
+        }
+        if (valid && q == 0) {
+            float4 yv;
+            if (!LAK) {
+                float4 acc = f4_zero();
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc = f4_add(acc, nb[j]);
-            yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(c2, 2.0f), 4.0f));
+                for (int j = 0; j < 4; ++j) acc = f4_add(acc, nb[j]);
+                yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(c2, 2.0f), 4.0f));
 #pragma unroll
-            for (int j = 0; j < 4; ++j) yv = f4_add(yv, f4_div(fq[j], 16.0f));
-        } else {
-            float4 acc = f4_zero();
+                for (int j = 0; j < 4; ++j) yv = f4_add(yv, f4_div(fq[j], 16.0f));
+            } else {
+                float4 acc = f4_zero();
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc = f4_add(acc, fq[j]);
+                for (int j = 0; j < 4; ++j) acc = f4_add(acc, fq[j]);
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
+                for (int r = 0; r < 4; ++r) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    int rk = 0;
+                    for (int j = 0; j < 4; ++j) {
+                        int rk = 0;
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) rk += tl[i] < tl[j];
-                    if (rk == r) acc = f4_add(acc, nb[j]);
+                        for (int i = 0; i < 4; ++i) rk += tl[i] < tl[j];
+                        if (rk == r) acc = f4_add(acc, nb[j]);
+                    }
                 }
+                yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(c2, 2.0f)), 4.0f);
             }
-            yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(c2, 2.0f)), 4.0f);
+            st4(R, (int64_t)d.V1 + (x >> 2), yv);
         }
-        st4(R, (int64_t)d.V1 + (x >> 2), yv);
-    }
 
-    // SLAK edge point N1 + x: half-edges 4x+2 (tail f, quad x) and 4 prev(x)+1 (tail e_in(x), quad prev x)
+        // SLAK edge point N1 + x: half-edges 4x+2 (tail f, quad x) and 4 prev(x)+1 (tail e_in(x), quad prev x)
+        if (!LAK) {
+            const float4 fprev = shfl4(fp, lp);
+            if (valid) {
+                float4 ta = f4_mul(f4_add(c2, fp), 0.25f);
+                float4 tb = f4_mul(f4_add(c3, fprev), 0.25f);
+                st4_cs(R, (int64_t)VFc + d.N1 + x, f4_add(f4_add(f4_zero(), ta), tb));
+            }
+        }
+
+        if (STATE && valid) {
+            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, qnext(tw1x), qnext(tw1_px), s1, t1x, eidp_x, eidp_px);
+            if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// GF (polygon P only): one thread per face g of P, with k corners x = ptr[g] ..
+// ptr[g+1]-1.  The vertex point of P's face point V1 + g (its column in C is
+// corners 4x+2, ascending) and, for SLAK, the edge points N1 + x of C's inner
+// edges {face point, e_in(x)}: the work k_g1 does with shuffles when P's faces
+// are quads.  Same formulas and order, with n = k.
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
+                                               const float* __restrict__ P, QState c, float* __restrict__ R)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= d.F1) return;
+    const int b = __ldg(pptr + g), e = __ldg(pptr + g + 1), k = e - b;
+    const float4 c2 = ldg4(P, d.V1 + g);
+    const float* FP = R + 4 * (int64_t)d.V;
+    const float nn = (float)(k * k);
+    float4 yv, acc = f4_zero();
     if (!LAK) {
-        const float4 fprev = shfl4(fp, lp);
-        if (valid) {
-            float4 ta = f4_mul(f4_add(c2, fp), 0.25f);
-            float4 tb = f4_mul(f4_add(c3, fprev), 0.25f);
-            st4_cs(R, (int64_t)VFc + d.N1 + x, f4_add(f4_add(f4_zero(), ta), tb));
+        for (int x = b; x < e; ++x) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * (int64_t)x + 3)));   // e_in(x)
+        yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(c2, (float)(k - 2)), (float)k));
+        for (int x = b; x < e; ++x) yv = f4_add(yv, f4_div(ldg4(FP, x), nn));
+        const int64_t VFc = (int64_t)d.V + d.N1;
+        for (int x = b; x < e; ++x) {
+            const int px = x == b ? e - 1 : x - 1;
+            const float4 ta = f4_mul(f4_add(c2, ldg4(FP, x)), 0.25f);
+            const float4 tb = f4_mul(f4_add(ldg4(P, __ldg(ids + 4 * (int64_t)x + 3)), ldg4(FP, px)), 0.25f);
+            st4_cs(R, VFc + d.N1 + x, f4_add(f4_add(f4_zero(), ta), tb));
         }
+    } else {
+        for (int x = b; x < e; ++x) acc = f4_add(acc, ldg4(FP, x));
+        // the tails e_out(x) in ascending id
+        int last = -1;
+        while (true) {
+            int xm = INT32_MAX;
+            for (int x = b; x < e; ++x) {
+                const int ti = __ldg(ids + 4 * (int64_t)x + 1);
+                if (ti > last && ti < xm) xm = ti;
+            }
+            if (xm == INT32_MAX) break;
+            acc = f4_add(acc, ldg4(P, xm));
+            last = xm;
+        }
+        yv = f4_div_z(f4_add(f4_div_z(acc, (float)k), f4_mul(c2, __fadd_rn((float)k, -2.0f))), (float)k);
     }
-
-    if (STATE && valid) {
-        // C's slot / twin / t for corners 4x+k
-        const int px = qprev(x), nxx = qnext(x);
-        const int ntw = qnext(tw1x), ntwp = qnext(tw1_px);
-        // edge of P through x: corners A=4x+1, B=4tw1x+1, Cc=4nxx+3, D=4ntw+3
-        const int A = 4 * x + 1, B = 4 * tw1x + 1, Cc = 4 * nxx + 3, D = 4 * ntw + 3;
-        // edge of P through prev(x): A'=4px+1, B'=4tw1_px+1, C'=4x+3, D'=4ntwp+3
-        const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
-        const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
-        reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
-        reinterpret_cast<int4*>(c.slot)[x] =
-            make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
-        if (!LAK)
-            reinterpret_cast<int4*>(c.t)[x] =
-                make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
-        if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
-    }
+    st4(R, (int64_t)d.V1 + g, yv);
+    if (STATE) c.sptr[d.V1 + g] = d.N1 + b;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -231,9 +316,10 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, const int* __restrict
 // of quads h and next(h)) are coalesced loads or shuffles, and only the twin
 // face's three (its face point, C's face points of quads h2 and next(h2)) are
 // gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
-template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict__ ids, const float* __restrict__ P,
-                                               QState p, QState c, float* __restrict__ R)
+template <bool LAK, bool STATE, bool PQ>
+__global__ void __launch_bounds__(kBlock) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                               const float* __restrict__ P, QState p, QState c,
+                                               float* __restrict__ R)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = x < d.N1;
@@ -244,12 +330,23 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, const int* __restrict
     const int4 Q = valid ? __ldg(reinterpret_cast<const int4*>(ids) + x) : make_int4(0, 0, 0, 0);
     const int h2 = valid ? __ldg(p.tw + x) : 0;
     const float4 Fh = valid ? ldg4(FP, x) : f4_zero();
-    const int u = __shfl_sync(0xffffffffu, Q.x, ln);
-    const float4 Fnh = shfl4(Fh, ln);
+    int u, nh;
+    float4 Fnh;
+    if (PQ) {
+        nh = qnext(x);
+        u = __shfl_sync(0xffffffffu, Q.x, ln);
+        Fnh = shfl4(Fh, ln);
+    } else {
+        if (!valid) return;
+        const int f = Q.z - d.V1, fb = __ldg(pf.ptr + f), fe = __ldg(pf.ptr + f + 1);
+        nh = x + 1 == fe ? fb : x + 1;
+        u = __ldg(ids + 4 * (int64_t)nh);
+    }
     if (!valid || Q.x >= u) return;              // not the min->max half-edge of its edge
-    const int h = x, nh = qnext(h), nh2 = qnext(h2);
+    if (!PQ) Fnh = ldg4(FP, nh);
+    const int h = x, nh2 = pf.next(h2);
     const int ve = Q.y, e = Q.y - d.V1 - d.F1;
-    const int fh = Q.z, fh2 = d.V1 + (h2 >> 2);
+    const int fh = Q.z, fh2 = d.V1 + pf.face(h2);
     const float4 Pv = ldg4(P, Q.x), Pu = ldg4(P, u);
     const float4 Pe = ldg4(P, ve), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2);
     const float4 Fh2 = ldg4(FP, h2), Fnh2 = ldg4(FP, nh2);
@@ -416,11 +513,13 @@ __global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const float* __restri
 
 // ---------------------------------------------------------------------------------------------
 // t of a general quad level feeding the fast path (SLAK): t[x] = slot[tw[prev x]]
-__global__ void k_export_t(int N, const int* __restrict__ slot, const int* __restrict__ tw, int* __restrict__ t)
+template <bool QUAD>
+__global__ void k_export_t(Faces<QUAD> fc, int N, const int* __restrict__ slot, const int* __restrict__ tw,
+                           int* __restrict__ t)
 {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= N) return;
-    t[x] = slot[tw[qprev(x)]];
+    t[x] = slot[tw[fc.prev(x)]];
 }
 
 }  // namespace slak

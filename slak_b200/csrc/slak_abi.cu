@@ -289,8 +289,8 @@ void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevSt
 }
 
 // One fast level: C = L (refined from its parent level Pl, whose state is L.in_state).
-template <bool LAK, bool STATE>
-void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
+template <bool LAK, bool STATE, bool PQ>
+void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc& lc)
 {
     FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N};
     cudaStream_t str = lc.s;
@@ -298,26 +298,39 @@ void launch_fast_t(const Level& Pl, const Level& L, bool comp, Lc& lc)
     // must read once, and the refined ids / positions it alone writes
     const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
-    k_g1<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state,
-                                                         reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots);
+    k_g1<LAK, STATE, PQ><<<grid_for(L.F), kBlock, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
+                                                             reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots);
     lc.after("k_g1", 1, g1b);
-    k_g2<LAK, STATE><<<grid_for(L.F), kBlock, 0, str>>>(d, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+    if (!PQ) {
+        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts);
+        lc.after("k_gf");
+    }
+    k_g2<LAK, STATE, PQ><<<grid_for(L.F), kBlock, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
+                                                             L.o_verts);
     lc.after("k_g2", 1, g2b);
     k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
                                                              L.o_verts, comp ? 1 : 0);
     lc.after("k_g3", 1, 16 * Pl.V + (LAK ? 0 : 16 * L.F));
 }
 
-void launch_fast(const Level& Pl, const Level& L, int scheme, bool comp, Lc& lc)
+template <bool PQ>
+void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool comp, Lc& lc)
+{
+    if (lak) {
+        if (L.make_state) launch_fast_t<true, true, PQ>(Pl, L, pf, comp, lc);
+        else launch_fast_t<true, false, PQ>(Pl, L, pf, comp, lc);
+    } else {
+        if (L.make_state) launch_fast_t<false, true, PQ>(Pl, L, pf, comp, lc);
+        else launch_fast_t<false, false, PQ>(Pl, L, pf, comp, lc);
+    }
+}
+
+// `cface` is the parent's corner -> face map when the parent is a polygon level
+void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, bool comp, Lc& lc)
 {
     const bool lak = scheme == SLAK_SCHEME_LAK;
-    if (lak) {
-        if (L.make_state) launch_fast_t<true, true>(Pl, L, comp, lc);
-        else launch_fast_t<true, false>(Pl, L, comp, lc);
-    } else {
-        if (L.make_state) launch_fast_t<false, true>(Pl, L, comp, lc);
-        else launch_fast_t<false, false>(Pl, L, comp, lc);
-    }
+    if (Pl.quad) launch_fast_p<true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else launch_fast_p<false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     if (L.o_ptr) {   // LAK final level: quad offsets and corner positions
         k_quad_ptr_vals<<<grid_for(L.N), kBlock, 0, lc.s>>>((int)L.N, L.o_ptr, reinterpret_cast<int4*>(L.o_vals));
         lc.after("k_quad_ptr_vals");
@@ -344,7 +357,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         const Level& L = p->lv[li];
         lc.level = (int)li;
         if (L.fast) {
-            launch_fast(p->lv[li - 1], L, p->scheme, comp, lc);
+            launch_fast(p->lv[li - 1], L, p->s.cface, p->scheme, comp, lc);
             continue;
         }
         launch_topology_a(L, (int)li, p->scheme, p->s, p->st, lc);
@@ -354,7 +367,12 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, lc);
         else launch_rest<false>(L, p->scheme, comp, p->s, p->st, lc);
         if (L.export_state && p->scheme == SLAK_SCHEME_SLAK) {   // slot / twin came from k_vsort / k_edges
-            k_export_t<<<grid_for(L.N), kBlock, 0, str>>>((int)L.N, p->s.xslot, p->s.xtw, p->s.xt);
+            if (L.quad)
+                k_export_t<true><<<grid_for(L.N), kBlock, 0, str>>>(Faces<true>{L.ptr, p->s.cface}, (int)L.N,
+                                                                    p->s.xslot, p->s.xtw, p->s.xt);
+            else
+                k_export_t<false><<<grid_for(L.N), kBlock, 0, str>>>(Faces<false>{L.ptr, p->s.cface}, (int)L.N,
+                                                                     p->s.xslot, p->s.xtw, p->s.xt);
             lc.after("k_export_t");
         }
     }
@@ -475,7 +493,7 @@ int plan_levels(slak_plan* p)
             L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
             L.E = (L.N - L.B) / 2 + L.B;
             L.quad = true; L.poly_fn = false;
-            L.fast = !force_general && P.quad && P.B == 0;
+            L.fast = !force_general && P.B == 0;     // closed parent, quad or polygon faces
         }
         L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
         if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
