@@ -153,10 +153,19 @@ def run_ours(args, dist, rank, ws):
     dev = torch.cuda.current_device()
     stream = torch.cuda.Stream()
     dm = api.DeviceMesh.from_host(mesh)
-    flags = api._abi.PLAN_GRAPH
+    flags = api._abi.PLAN_GRAPH | (0 if args.no_tune else api._abi.PLAN_AUTOTUNE)
     with torch.cuda.stream(stream):
-        plan = api.Plan(dm, levels, scheme, flags, stream=stream)
+        plan = api.Plan(dm, levels, scheme, flags, stream=stream)     # tuning runs here, untimed
     stats = plan.level_stats()
+    tuning = []
+    for t in plan.tuning():
+        if t["state"] < 0:
+            continue
+        row = {"level": t["level"], "key": t["key"], "block": t["block"], "state": t["state"]}
+        if t["state"] == 1:    # measured now: each kernel's ms at its choice and at the default 256
+            row["ms_chosen"] = [t["ms"][k][(128, 256, 512).index(t["block"][k])] for k in range(3)]
+            row["ms_block256"] = [t["ms"][k][1] for k in range(3)]
+        tuning.append(row)
     faces = stats[-1]["out_faces"]
     alg_bytes = sum(s["algorithmic_bytes"] for s in stats)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -218,6 +227,7 @@ def run_ours(args, dist, rank, ws):
         "roofline": kern,
         "kernels": ktable[:8],
         "levels": per_level,
+        "tuning": tuning,
         "pipeline_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                               "frac": achieved / peak, "peak_kind": peak_kind,
                               "algorithmic_bytes": alg_bytes},
@@ -394,7 +404,8 @@ def run_batch(args, torch, dist, rank, ws):
 
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
-        b = api.Batch(dms, [l for _, l in items], scheme, api._abi.PLAN_GRAPH, stream=stream)
+        b = api.Batch(dms, [l for _, l in items], scheme,
+                      api._abi.PLAN_GRAPH | (0 if args.no_tune else api._abi.PLAN_AUTOTUNE), stream=stream)
     create_s = time.perf_counter() - t0
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     dev = torch.cuda.current_device()
@@ -494,6 +505,7 @@ def main():
     ap.add_argument("--workload", default="mixed512")
     ap.add_argument("--scheme", default="slak", choices=["slak", "lak"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--batch-count", type=int, default=2000)
     ap.add_argument("--batch-plain-reps", type=int, default=1)

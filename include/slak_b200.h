@@ -148,7 +148,8 @@ enum slak_plan_flags {
     SLAK_PLAN_GRAPH = 1,        /* capture one execution as a CUDA graph and replay it       */
     SLAK_PLAN_GENERAL = 2,      /* run every level through the general per-level path         */
     SLAK_PLAN_COMPENSATED = 4,  /* compensated (TwoSum) sums in high-valence vertex points    */
-    SLAK_PLAN_TIMING = 8        /* record a CUDA event after every launch (per-kernel times)  */
+    SLAK_PLAN_TIMING = 8,       /* record a CUDA event after every launch (per-kernel times)  */
+    SLAK_PLAN_AUTOTUNE = 16     /* measure launch shapes of untuned keys at creation (below)  */
 };
 
 typedef struct slak_kernel_timing {
@@ -157,6 +158,15 @@ typedef struct slak_kernel_timing {
     float ms;                   /* device time since the previous launch's event   */
     int64_t algorithmic_bytes;  /* compulsory bytes it moves, 0 when not defined    */
 } slak_kernel_timing;
+
+/* Launch shapes of one fast level (slak_plan_tuning). */
+typedef struct slak_tuning {
+    int32_t state;              /* -1 not a fast level, 0 default, 1 measured by this plan,
+                                   2 taken from the tuning cache                         */
+    int32_t block[3];           /* block size of k_g1, k_g2, k_g3                          */
+    float ms[3][3];             /* state 1: median ms of each kernel at block 128/256/512  */
+    char key[64];               /* tuning-cache key                                        */
+} slak_tuning;
 
 typedef struct slak_level_stats {
     int64_t nfaces, nverts, nnz, nedges, nboundary;   /* of the level's input mesh */
@@ -179,6 +189,20 @@ int64_t slak_plan_launches(const slak_plan* plan);
  * (waits for it); returns the number of launches, or -status. */
 int slak_plan_kernel_timings(slak_plan* plan, slak_kernel_timing* out, int capacity);
 int slak_plan_destroy(slak_plan* plan);
+
+/*
+ * Autotuner (no counterpart in the reference, whose launch shapes are fixed).
+ * The block sizes of the three closed-form kernels of every fast level are
+ * chosen by measurement, keyed on the scheme, the parent level's face type,
+ * whether the level feeds another fast level, log2 of the level's quads and
+ * the input's valence histogram (largest valence; share of valence 4).  Every
+ * plan and batch applies cached choices; with SLAK_PLAN_AUTOTUNE, creation also
+ * measures the keys not yet cached (block 128 / 256 / 512 per kernel, median of
+ * three executions).  The cache lives in the process; with SLAK_TUNE_FILE set
+ * in the environment it is also loaded from and saved to that file.
+ */
+int slak_plan_tuning(const slak_plan* plan, int level, slak_tuning* out);
+int slak_autotune_reset(void);    /* forget the in-process cache (the file is kept) */
 
 /*
  * Batches: many meshes, each with its own target level, refined by one call

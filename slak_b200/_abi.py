@@ -14,13 +14,14 @@ SLAK_OK = 0
 STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: "SLAK_ERR_OOM",
                 4: "SLAK_ERR_BAD_MESH", 5: "SLAK_ERR_TIMEOUT", 6: "SLAK_ERR_UNSUPPORTED", 7: "SLAK_ERR_NOT_READY"}
 
-PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING = 1, 2, 4, 8
+PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4, 8, 16
 
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
            "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
+           "slak_plan_tuning", "slak_autotune_reset",
            "slak_plan_destroy", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
            "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
 
@@ -43,6 +44,11 @@ class LevelStats(ctypes.Structure):
 class KernelTiming(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char_p), ("level", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("algorithmic_bytes", ctypes.c_int64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("block", ctypes.c_int32 * 3), ("ms", (ctypes.c_float * 3) * 3),
+                ("key", ctypes.c_char * 64)]
 
 
 class SlakError(RuntimeError):
@@ -87,6 +93,10 @@ def lib():
         L.slak_plan_destroy.argtypes = [V]
         L.slak_plan_kernel_timings.argtypes = [V, ctypes.POINTER(KernelTiming), I]
         L.slak_plan_kernel_timings.restype = I
+        L.slak_plan_tuning.argtypes = [V, I, ctypes.POINTER(Tuning)]
+        L.slak_plan_tuning.restype = I
+        L.slak_autotune_reset.argtypes = []
+        L.slak_autotune_reset.restype = I
         L.slak_batch_create.argtypes = [P, ctypes.POINTER(ctypes.c_int), I64, I, I, V, ctypes.POINTER(V)]
         L.slak_batch_execute.argtypes = [V, V]
         L.slak_batch_status.argtypes = [V, V]

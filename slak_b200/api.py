@@ -195,6 +195,18 @@ class Plan:
         return [{"name": buf[i].name.decode(), "level": int(buf[i].level), "ms": float(buf[i].ms),
                  "algorithmic_bytes": int(buf[i].algorithmic_bytes)} for i in range(n)]
 
+    def tuning(self) -> List[dict]:
+        """Launch shapes of every level (slak_plan_tuning): state -1 for a
+        general level, 0 default, 1 measured by this plan, 2 from the cache."""
+        out = []
+        for i in range(_abi.lib().slak_plan_num_levels(self._h)):
+            t = _abi.Tuning()
+            _abi.check(_abi.lib().slak_plan_tuning(self._h, i, ctypes.byref(t)), "slak_plan_tuning")
+            out.append({"level": i, "state": int(t.state), "block": list(t.block),
+                        "ms": [[float(t.ms[k][c]) for c in range(3)] for k in range(3)],
+                        "key": t.key.decode()})
+        return out
+
     def level_stats(self) -> List[dict]:
         out = []
         for i in range(_abi.lib().slak_plan_num_levels(self._h)):

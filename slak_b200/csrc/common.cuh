@@ -112,6 +112,7 @@ struct DevStatus {
     int nextern;      // boundary half-edges of level 0
     int nedges;       // edges of level 0
     int bcount[32];   // boundary half-edges counted per level
+    int vhist[17];    // level 0: vertices of valence 0..15, and 16 or more
 };
 
 __device__ __forceinline__ void set_error(DevStatus* st, int code, int detail)

@@ -107,12 +107,12 @@ __device__ __forceinline__ void write_state(const FastDims& d, QState& c, int x,
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
-template <bool LAK, bool STATE, bool PQ>
-__global__ void __launch_bounds__(kBlock) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                               const float* __restrict__ P, QState p, QState c,
-                                               int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
+template <bool LAK, bool STATE, bool PQ, int BS>
+__global__ void __launch_bounds__(BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                           const float* __restrict__ P, QState p, QState c,
+                                           int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
-    __shared__ int4 sq[4 * kBlock];
+    __shared__ int4 sq[4 * BS];
     const int x0 = blockIdx.x * blockDim.x;
     const int x = x0 + threadIdx.x;
     const bool valid = x < d.N1;
@@ -182,11 +182,11 @@ __global__ void __launch_bounds__(kBlock) k_g1(FastDims d, Faces<PQ> pf, const i
     sq[4 * threadIdx.x + 3] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
     __syncthreads();
     {
-        const int nq = min(kBlock, d.N1 - x0);
+        const int nq = min(BS, d.N1 - x0);
         int4* dst = out_ids + 4 * (int64_t)x0;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int j = i * kBlock + threadIdx.x;
+            const int j = i * BS + threadIdx.x;
             if (j < 4 * nq) __stcs(dst + j, sq[j]);
         }
     }
@@ -316,10 +316,9 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
 // of quads h and next(h)) are coalesced loads or shuffles, and only the twin
 // face's three (its face point, C's face points of quads h2 and next(h2)) are
 // gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
-template <bool LAK, bool STATE, bool PQ>
-__global__ void __launch_bounds__(kBlock) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                               const float* __restrict__ P, QState p, QState c,
-                                               float* __restrict__ R)
+template <bool LAK, bool STATE, bool PQ, int BS>
+__global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                           const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = x < d.N1;
@@ -401,9 +400,9 @@ __global__ void __launch_bounds__(kBlock) k_g2(FastDims d, Faces<PQ> pf, const i
 // G3: one thread per vertex v of P.  Its column's records (written by k_g1 at
 // the column's slots) are contiguous, so the vertex point and, for SLAK, the
 // edge points of C's edges {v, e_out(x)} (ids = the slots) stream.
-template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
-                                               SlotScratch z, float* __restrict__ R, int compensated)
+template <bool LAK, bool STATE, int BS>
+__global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
+                                           SlotScratch z, float* __restrict__ R, int compensated)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= d.V1) {

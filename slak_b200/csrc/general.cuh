@@ -46,6 +46,19 @@ __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __rest
     atomicAdd(cnt + v, 1);
 }
 
+// valence histogram (0..15, 16 or more): the autotuner's key, read with the
+// level-0 probe
+__global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restrict__ hist)
+{
+    __shared__ int h[17];
+    if (threadIdx.x < 17) h[threadIdx.x] = 0;
+    __syncthreads();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V) atomicAdd(&h[min(sptr[v + 1] - sptr[v], 16)], 1);
+    __syncthreads();
+    if (threadIdx.x < 17 && h[threadIdx.x]) atomicAdd(hist + threadIdx.x, h[threadIdx.x]);
+}
+
 // slot order from the atomic is arbitrary (the unsorted column goes to
 // `loose`); k_vsort makes it canonical
 __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,

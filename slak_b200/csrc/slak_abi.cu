@@ -17,6 +17,10 @@
 #include <new>
 #include <vector>
 #include <algorithm>
+#include <array>
+#include <cmath>
+#include <map>
+#include <type_traits>
 
 #include "common.cuh"
 #include "general.cuh"
@@ -44,7 +48,23 @@ struct Level {
     float* o_verts = nullptr;
     int* o_ptr = nullptr;
     int* o_vals = nullptr;
+    // fast level: block size of k_g1, k_g2, k_g3 (chosen by the autotuner)
+    int bs[3] = {256, 256, 256};
+    int tuned = 0;                 // 0 default, 1 measured now, 2 from the tuning cache
+    float tune_ms[3][3] = {};      // measured ms of each kernel at block 128 / 256 / 512
+    std::string tune_key;
 };
+
+constexpr int kTuneBlocks[3] = {128, 256, 512};
+
+// Calls f with the block size as a compile-time constant.
+template <class F>
+void with_block(int bs, F&& f)
+{
+    if (bs == 128) f(std::integral_constant<int, 128>{});
+    else if (bs == 512) f(std::integral_constant<int, 512>{});
+    else f(std::integral_constant<int, 256>{});
+}
 
 struct Scratch {
     int *cface = nullptr, *cnt = nullptr, *sptr = nullptr, *sc = nullptr, *snext = nullptr, *sprev = nullptr,
@@ -143,6 +163,7 @@ struct slak_plan {
     int64_t launches = 0;
     int executed = 0;
     bool debug = false;
+    int vhist[17] = {};              // level 0's valence histogram (probe)
     // per-launch timing (SLAK_PLAN_TIMING)
     std::vector<cudaEvent_t> ev;
     std::vector<KernelRec> recs;
@@ -298,18 +319,28 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     // must read once, and the refined ids / positions it alone writes
     const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
-    k_g1<LAK, STATE, PQ><<<grid_for(L.F), kBlock, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
-                                                             reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots);
+    with_block(L.bs[0], [&](auto b) {
+        constexpr int BS = decltype(b)::value;
+        k_g1<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
+                                                                    reinterpret_cast<int4*>(L.o_ids), L.o_verts,
+                                                                    L.slots);
+    });
     lc.after("k_g1", 1, g1b);
     if (!PQ) {
         k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts);
         lc.after("k_gf");
     }
-    k_g2<LAK, STATE, PQ><<<grid_for(L.F), kBlock, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
-                                                             L.o_verts);
+    with_block(L.bs[1], [&](auto b) {
+        constexpr int BS = decltype(b)::value;
+        k_g2<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
+                                                                    L.o_verts);
+    });
     lc.after("k_g2", 1, g2b);
-    k_g3<LAK, STATE><<<grid_for(Pl.V + 1), kBlock, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
-                                                             L.o_verts, comp ? 1 : 0);
+    with_block(L.bs[2], [&](auto b) {
+        constexpr int BS = decltype(b)::value;
+        k_g3<LAK, STATE, BS><<<grid_for(Pl.V + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
+                                                                     L.o_verts, comp ? 1 : 0);
+    });
     lc.after("k_g3", 1, 16 * Pl.V + (LAK ? 0 : 16 * L.F));
 }
 
@@ -429,6 +460,7 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str, void* given = nullpt
     Lc lc{str, &nl, p->debug, 0};
     cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
     launch_topology_a(L0, 0, p->scheme, s, st, lc);
+    k_valence_hist<<<grid_for(L0.V), kBlock, 0, str>>>((int)L0.V, s.sptr, st->vhist);
     cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
@@ -438,6 +470,7 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str, void* given = nullpt
     if (p->h_st->err) { g_detail = "level-0 probe: device detail " + std::to_string(p->h_st->detail); return p->h_st->err; }
     L0.B = p->h_st->bcount[0];
     L0.E = p->h_st->nedges;
+    std::memcpy(p->vhist, p->h_st->vhist, sizeof(p->vhist));
     if (L0.E != (L0.N - L0.B) / 2 + L0.B) return SLAK_ERR_BAD_MESH;   // not a 2-manifold
     return SLAK_OK;
 }
@@ -635,6 +668,140 @@ cudaError_t workspace_reserve(Workspace* w, size_t bytes)
 
 }  // namespace
 
+// ------------------------------------------------------------------ autotuner
+// The block sizes of k_g1 / k_g2 / k_g3 of every fast level are chosen by
+// measurement.  The key is what sets them: the scheme, the parent's face type,
+// whether the level writes the next level's state, the level's size (log2 of
+// its quads) and the input's valence histogram (largest valence class; share
+// of valence-4 vertices).  Choices are cached per process and, with
+// SLAK_TUNE_FILE set, in that text file (a key and three block sizes a line).
+// Every plan applies cached choices; SLAK_PLAN_AUTOTUNE measures missing keys.
+std::mutex g_tune_mu;
+std::map<std::string, std::array<int, 3>> g_tune;
+bool g_tune_loaded = false;
+const char* const kTuneKernels[3] = {"k_g1", "k_g2", "k_g3"};
+
+std::string tune_key(const slak_plan* p, int li)
+{
+    const Level& L = p->lv[li];
+    const Level& P = p->lv[li - 1];
+    int vmax = 0;
+    int64_t tot = 0;
+    for (int k = 0; k < 17; ++k) {
+        if (p->vhist[k]) vmax = k;
+        tot += p->vhist[k];
+    }
+    const double share4 = tot ? (double)p->vhist[4] / (double)tot : 0.0;
+    const int vclass = vmax <= 4 ? 4 : vmax <= 8 ? 8 : vmax < 16 ? 15 : 16;
+    const int sclass = share4 < 0.5 ? 0 : share4 < 0.9 ? 50 : 90;
+    const int fb = (int)std::floor(std::log2((double)std::max<int64_t>(L.F, 1)));
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "%s/%s/%s/q2^%d/vmax%d/v4_%d", p->scheme == SLAK_SCHEME_LAK ? "lak" : "slak",
+                  P.quad ? "quad" : "poly", L.make_state ? "state" : "last", fb, vclass, sclass);
+    return buf;
+}
+
+bool valid_block(int b) { return b == 128 || b == 256 || b == 512; }
+
+void tune_load_locked()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("SLAK_TUNE_FILE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[128];
+    int a, b, c;
+    while (std::fscanf(f, "%127s %d %d %d", key, &a, &b, &c) == 4)
+        if (valid_block(a) && valid_block(b) && valid_block(c)) g_tune[key] = {a, b, c};
+    std::fclose(f);
+}
+
+void tune_save_locked()
+{
+    const char* path = std::getenv("SLAK_TUNE_FILE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return;
+    for (const auto& kv : g_tune) std::fprintf(f, "%s %d %d %d\n", kv.first.c_str(), kv.second[0], kv.second[1], kv.second[2]);
+    std::fclose(f);
+}
+
+// cached choices for every fast level; returns the fast levels still untuned
+std::vector<int> apply_tuning(slak_plan* p)
+{
+    std::vector<int> todo;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    for (int i = 1; i < (int)p->lv.size(); ++i) {
+        Level& L = p->lv[i];
+        if (!L.fast) continue;
+        L.tune_key = tune_key(p, i);
+        auto it = g_tune.find(L.tune_key);
+        if (it != g_tune.end()) {
+            for (int k = 0; k < 3; ++k) L.bs[k] = it->second[k];
+            L.tuned = 2;
+        } else {
+            todo.push_back(i);
+        }
+    }
+    return todo;
+}
+
+// device ms of kernel `name` of level `li` in the last timed execution
+float kernel_ms(slak_plan* p, int li, const char* name)
+{
+    for (size_t i = 0; i < p->recs.size(); ++i)
+        if (p->recs[i].level == li && std::strcmp(p->recs[i].name, name) == 0) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]);
+            return ms;
+        }
+    return 0.f;
+}
+
+// Measures every candidate block size of each kernel of the untuned fast
+// levels (median of 3 timed executions each; the other kernels keep their
+// current choice) and keeps the fastest.  Runs the plan eagerly several
+// times; its outputs are rewritten by the next execution.
+int plan_autotune(slak_plan* p, cudaStream_t str)
+{
+    std::vector<int> todo = apply_tuning(p);
+    if (todo.empty()) return SLAK_OK;
+    const int saved = p->flags;
+    p->flags |= SLAK_PLAN_TIMING;
+    int rc = enqueue_all(p, str);                          // warm-up
+    if (rc == SLAK_OK) rc = cuda_status(cudaStreamSynchronize(str));
+    for (int li : todo) {
+        Level& L = p->lv[li];
+        for (int k = 0; k < 3 && rc == SLAK_OK; ++k) {
+            for (int ci = 0; ci < 3 && rc == SLAK_OK; ++ci) {
+                L.bs[k] = kTuneBlocks[ci];
+                float t[3] = {0.f, 0.f, 0.f};
+                for (int r = 0; r < 3 && rc == SLAK_OK; ++r) {
+                    rc = enqueue_all(p, str);
+                    if (rc == SLAK_OK) rc = cuda_status(cudaStreamSynchronize(str));
+                    t[r] = kernel_ms(p, li, kTuneKernels[k]);
+                }
+                std::sort(t, t + 3);
+                L.tune_ms[k][ci] = t[1];
+            }
+            int best = 1;                                   // ties keep the default
+            for (int ci = 0; ci < 3; ++ci)
+                if (L.tune_ms[k][ci] < L.tune_ms[k][best]) best = ci;
+            L.bs[k] = kTuneBlocks[best];
+        }
+        L.tuned = 1;
+    }
+    p->flags = saved;
+    if (rc != SLAK_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int li : todo) g_tune[p->lv[li].tune_key] = {p->lv[li].bs[0], p->lv[li].bs[1], p->lv[li].bs[2]};
+    tune_save_locked();
+    return SLAK_OK;
+}
+
 // Plan creation; with `ws`, the arena and the status word come from the
 // workspace (the plan does not own them).
 static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, int flags, cudaStream_t str,
@@ -683,6 +850,9 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
     p->out = o;
     if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
     plan_wire(p);
+    if (flags & SLAK_PLAN_AUTOTUNE) rc = plan_autotune(p, str);
+    else apply_tuning(p);
+    if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
     *out_plan = p;
     return SLAK_OK;
 }
@@ -807,6 +977,28 @@ int slak_plan_kernel_timings(slak_plan* p, slak_kernel_timing* out, int capacity
         out[i].algorithmic_bytes = p->recs[i].bytes;
     }
     return n;
+}
+
+int slak_plan_tuning(const slak_plan* p, int level, slak_tuning* out)
+{
+    if (!p || !out || level < 0 || level >= (int)p->lv.size()) return SLAK_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof(*out));
+    const Level& L = p->lv[level];
+    out->state = L.fast ? L.tuned : -1;
+    for (int k = 0; k < 3; ++k) {
+        out->block[k] = L.bs[k];
+        for (int c = 0; c < 3; ++c) out->ms[k][c] = L.tune_ms[k][c];
+    }
+    std::snprintf(out->key, sizeof out->key, "%s", L.tune_key.c_str());
+    return SLAK_OK;
+}
+
+int slak_autotune_reset(void)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.clear();
+    g_tune_loaded = true;     // the file is not read again
+    return SLAK_OK;
 }
 
 int slak_plan_destroy(slak_plan* p)
@@ -1007,6 +1199,7 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
                 if (!p) continue;
                 cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
                 launch_topology_a(p->lv[0], 0, scheme, sc, st, lc);
+                k_valence_hist<<<grid_for(p->lv[0].V), kBlock, 0, str>>>((int)p->lv[0].V, sc.sptr, st->vhist);
                 cudaMemcpyAsync(&b->h_st[i], st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
                 cudaMemcpyAsync(&b->h_st[i].nedges, sc.eptr + p->lv[0].V, sizeof(int), cudaMemcpyDeviceToHost, str);
             }
@@ -1025,6 +1218,7 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
             Level& L0 = p->lv[0];
             L0.B = b->h_st[i].bcount[0];
             L0.E = b->h_st[i].nedges;
+            std::memcpy(p->vhist, b->h_st[i].vhist, sizeof(p->vhist));
             if (L0.E != (L0.N - L0.B) / 2 + L0.B) { g_detail = "mesh " + std::to_string(i); rc = SLAK_ERR_BAD_MESH; }
             else rc = plan_levels(p);
         }
@@ -1109,6 +1303,14 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
         for (auto& st2 : b->streams) cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
         ce = cudaGetLastError();
         if (ce != cudaSuccess) rc = cuda_status(ce);
+    }
+    // launch shapes: cached choices, or (SLAK_PLAN_AUTOTUNE) measured on the
+    // first mesh of each key, alone on `stream`, before any batch execution
+    for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+        slak_plan* p = b->plans[i];
+        if (!p) continue;
+        if (flags & SLAK_PLAN_AUTOTUNE) rc = plan_autotune(p, str);
+        else apply_tuning(p);
     }
     if (rc != SLAK_OK) { batch_free(b); return rc; }
     *out_batch = b;
