@@ -47,9 +47,6 @@ def test_reference_matches_oracle_small(case, scheme):
     name, mesh, levels = case
     if scheme == LAK and mesh.ptr is None:
         mesh = mesh.with_quad_ptr()
-    if scheme == SLAK and name in ("grid", "fan"):
-        # boundary corrections use 3/4 p + 1/8 q, which the reference's compiler may contract into an FMA
-        pass
     _compare(mesh, levels, scheme)
 
 
