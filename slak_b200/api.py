@@ -221,7 +221,10 @@ class Plan:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:       # interpreter teardown: the library may already be unloaded
+            pass
 
 
 def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0) -> HostResult:
@@ -282,4 +285,7 @@ class Batch:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:       # interpreter teardown: the library may already be unloaded
+            pass

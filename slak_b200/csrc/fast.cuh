@@ -76,13 +76,16 @@ __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a
 // as one contiguous 16 KB run.
 // Slot-ordered records for the per-vertex pass (k_g3): for the corner x of P
 // at slot s = slot1(x), Z[2s] = FP(x) and Z[2s+1] = the position of C's next
-// (SLAK: e_out(x)) or previous (LAK: e_in(x)) vertex of corner 4x; T[s] = that
-// vertex id (LAK ordering); B[t1(x)] = (P[e_in(x)] + FP(x)) / 4, the half of the
-// SLAK edge point t1(x) contributed by half-edge 4x+3.
+// (SLAK: e_out(x)) or previous (LAK: e_in(x)) vertex of corner 4x.  LAK:
+// T[s] = that vertex id (for the ascending-id order).  SLAK: rot[t1(x)] = s.
+// The corner y at slot t1(x) = slot1(tw(prev x)) is x's neighbour around their
+// vertex across the edge e_in(x) = e_out(y), so half-edge 4x+3's share of SLAK
+// edge point t1(x), (P[e_in(x)] + FP(x)) / 4, is (Z[2 t1(x) + 1] + Z[2 rot]) / 4:
+// two records of the same column, which k_g3 has loaded anyway.
 struct SlotScratch {
     float4* Z;
-    float4* B;
-    int* T;
+    int* T;      // LAK
+    int* rot;    // SLAK (the same memory as T: one scheme per plan)
 };
 
 // C's slot / twin / t for its corners 4x+k (the state the next fast level reads)
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(BS) k_g1(FastDims d, Faces<PQ> pf, const int* 
         z.Z[2 * (int64_t)s1] = fp;
         z.Z[2 * (int64_t)s1 + 1] = LAK ? c3 : c1;
         if (LAK) z.T[s1] = Q.w;
-        else z.B[t1x] = f4_mul(f4_add(c3, fp), 0.25f);
+        else z.rot[t1x] = s1;
     }
 
     if constexpr (!PQ) {
@@ -277,6 +280,60 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
     const float* FP = R + 4 * (int64_t)d.V;
     const float nn = (float)(k * k);
     float4 yv, acc = f4_zero();
+    if (k <= 8) {
+        // faces of up to 8 corners: every load issued up front (same arithmetic and order as below)
+        int vi[8];
+        float4 fq[8], pe[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < k) {
+                vi[j] = __ldg(ids + 4 * (int64_t)(b + j) + (LAK ? 1 : 3));    // LAK: e_out; SLAK: e_in
+                fq[j] = ldg4(FP, b + j);
+            }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < k) pe[j] = ldg4(P, vi[j]);
+        if (!LAK) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (j < k) acc = f4_add(acc, pe[j]);
+            yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(c2, (float)(k - 2)), (float)k));
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (j < k) yv = f4_add(yv, f4_div(fq[j], nn));
+            const int64_t VFc = (int64_t)d.V + d.N1;
+            float4 fprev = fq[0];
+#pragma unroll
+            for (int j = 1; j < 8; ++j)
+                if (j == k - 1) fprev = fq[j];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (j < k) {
+                    const float4 ta = f4_mul(f4_add(c2, fq[j]), 0.25f);
+                    const float4 tb = f4_mul(f4_add(pe[j], fprev), 0.25f);
+                    st4_cs(R, VFc + d.N1 + b + j, f4_add(f4_add(f4_zero(), ta), tb));
+                    fprev = fq[j];
+                }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (j < k) acc = f4_add(acc, fq[j]);
+            // the tails e_out(x) in ascending id (distinct within a face)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    int rk = 0;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) rk += (i < k && vi[i] < vi[j]);
+                    if (j < k && rk == r) acc = f4_add(acc, pe[j]);
+                }
+            yv = f4_div_z(f4_add(f4_div_z(acc, (float)k), f4_mul(c2, __fadd_rn((float)k, -2.0f))), (float)k);
+        }
+        st4(R, (int64_t)d.V1 + g, yv);
+        if (STATE) c.sptr[d.V1 + g] = d.N1 + b;
+        return;
+    }
     if (!LAK) {
         for (int x = b; x < e; ++x) acc = f4_add(acc, ldg4(P, __ldg(ids + 4 * (int64_t)x + 3)));   // e_in(x)
         yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(c2, (float)(k - 2)), (float)k));
@@ -417,15 +474,14 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
     if (n <= 4) {
         // the common case: every record of the column loaded up front (the
         // arithmetic and its order are the loops' below)
-        float4 zf[4], zn[4], bb[4];
-        int tt[4];
+        float4 zf[4], zn[4];
+        int tt[4];                             // LAK: tail ids; SLAK: rot - b
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k < n) {
                 zf[k] = __ldg(Z + 2 * (int64_t)(b + k));
                 zn[k] = __ldg(Z + 2 * (int64_t)(b + k) + 1);
-                if (!LAK) bb[k] = __ldg(z.B + b + k);
-                else tt[k] = __ldg(z.T + b + k);
+                tt[k] = LAK ? __ldg(z.T + b + k) : __ldg(z.rot + b + k) - b;
             }
         }
         float4 acc = f4_zero();
@@ -440,8 +496,12 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
             const int64_t EPb = (int64_t)d.V + d.N1;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (k < n)
-                    st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), f4_mul(f4_add(Pv, zf[k]), 0.25f)), bb[k]));
+                if (k < n) {
+                    const int r = tt[k];
+                    const float4 fr = r == 0 ? zf[0] : r == 1 ? zf[1] : r == 2 ? zf[2] : zf[3];
+                    const float4 half = f4_mul(f4_add(zn[k], fr), 0.25f);
+                    st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), f4_mul(f4_add(Pv, zf[k]), 0.25f)), half));
+                }
         } else {
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -478,11 +538,14 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
             for (int s = b; s < e; ++s) dd_acc(sh, sl, __ldg(Z + 2 * (int64_t)s));
             yv = vp_finish(sh, sl, Pv, n);
         }
-        // edge points of C's edges {v, e_out(x)}, ids b..e-1: 0 + (p_v + FP(x))/4 + B[s]
+        // edge points of C's edges {v, e_out(x)}, ids b..e-1:
+        // 0 + (p_v + FP(x))/4 + (Z[2s+1] + Z[2 rot[s]])/4
         const int64_t EPb = (int64_t)d.V + d.N1;
         for (int s = b; s < e; ++s) {
             const float4 ta = f4_mul(f4_add(Pv, __ldg(Z + 2 * (int64_t)s)), 0.25f);
-            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), __ldg(z.B + s)));
+            const float4 tb = f4_mul(f4_add(__ldg(Z + 2 * (int64_t)s + 1), __ldg(Z + 2 * (int64_t)__ldg(z.rot + s))),
+                                     0.25f);
+            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), tb));
         }
     } else {
         // face points in column order, then the tails e_in(x) in ascending id

@@ -564,8 +564,7 @@ void plan_carve(slak_plan* p, Carver& cv)
     if (p->stN) { carve_state(cv, p->qs[0], p->stN, p->stV); carve_state(cv, p->qs[1], p->stN, p->stV); }
     if (p->slN) {
         p->slots.Z = cv.take<float4>(2 * p->slN);
-        p->slots.B = cv.take<float4>(p->slN);
-        p->slots.T = cv.take<int>(p->slN);
+        p->slots.T = p->slots.rot = cv.take<int>(p->slN);
     }
     for (int k = 0; k < 2; ++k) {
         p->ping_ids[k] = nlev > 1 ? cv.take<int>(p->mid_ids) : nullptr;
