@@ -22,12 +22,15 @@
 //   LAK   edges around edge point e are 4e + {lower end, higher end,
 //         lower face point, higher face point}      [ascending (max, min)]
 //
-// Three kernels per level write every output exactly once, in contiguous runs:
-//   k_g1  per quad of C (4 threads per face of P): C's refined quads, face
-//         points of C, vertex points of the face points of P, SLAK edge points
-//         N1+x, and the next level's per-corner state
-//   k_g2  per edge of P, visited in corner order (the min->max half-edge's
-//         lane): vertex points of the edge points of P, LAK edge points
+// Two kernels per level when P has quad faces, four when P is the polygon
+// input; every output is written exactly once:
+//   k_g1  per quad of C: C's refined quads, face points of C and the next
+//         level's per-corner state; with quad P (4 lanes per face of P) also
+//         the vertex points of P's face and edge points, SLAK edge points N1+x
+//         and LAK's edge points
+//   k_gf  polygon P: per face of P, its face point's vertex point, SLAK N1+x
+//   k_g2  polygon P: per edge of P, visited in corner order (the min->max
+//         half-edge's lane): vertex points of P's edge points, LAK edge points
 //   k_g3  per vertex of P: vertex points of P's vertices and SLAK edge points
 //         slot1(x), streamed from slot-ordered records k_g1 scatters
 // The float arithmetic and its order are exactly the general path's (and the
@@ -107,6 +110,65 @@ __device__ __forceinline__ void write_state(const FastDims& d, QState& c, int x,
             make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
 }
 
+// The vertex point of P's edge point ve (edge e = ve - V1 - F1, half-edges
+// h: v->u, the min->max one, and h2: u->v) and, for LAK, the four edge points
+// 4e..4e+3 of C around it.  Inputs: the positions of v, u, ve and of the two
+// face points fh (of h's face), fh2 (of h2's); C's face points of quads h,
+// next(h), h2, next(h2).
+template <bool LAK, bool STATE>
+__device__ __forceinline__ void edge_point_vertex(const FastDims& d, QState& c, float* __restrict__ R, int h,
+                                                  int nh, int h2, int nh2, int ve, int fh, int fh2, float4 Pv,
+                                                  float4 Pu, float4 Pe, float4 Pf, float4 Pf2, float4 Fh, float4 Fnh,
+                                                  float4 Fh2, float4 Fnh2)
+{
+    const int e = ve - d.V1 - d.F1;
+    // corners of the edge point: A=4h+1 (nbr fh, face h), B=4h2+1 (fh2, h2), C=4nh+3 (u, nh), D=4nh2+3 (v, nh2)
+    const int A = 4 * h + 1, B = 4 * h2 + 1, Cc = 4 * nh + 3, D = 4 * nh2 + 3;
+    const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D);
+    float4 nb[4], fq[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        nb[r] = rA == r ? Pf : rB == r ? Pf2 : rC == r ? Pu : Pv;
+        fq[r] = rA == r ? Fh : rB == r ? Fh2 : rC == r ? Fnh : Fnh2;
+    }
+    float4 yv;
+    if (!LAK) {
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = f4_add(acc, nb[r]);
+        yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(Pe, 2.0f), 4.0f));
+#pragma unroll
+        for (int r = 0; r < 4; ++r) yv = f4_add(yv, f4_div(fq[r], 16.0f));
+    } else {
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = f4_add(acc, fq[r]);
+        // tails {v, u, fh, fh2} in ascending id: v < u < V1 <= fh, fh2
+        const bool ff = fh < fh2;
+        acc = f4_add(acc, Pv);
+        acc = f4_add(acc, Pu);
+        acc = f4_add(acc, ff ? Pf : Pf2);
+        acc = f4_add(acc, ff ? Pf2 : Pf);
+        yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(Pe, 2.0f)), 4.0f);
+    }
+    st4_cs(R, ve, yv);
+
+    if (LAK) {
+        // edges 4e + {lower end, higher end, lower face point, higher face point}; v < u
+        const float4 Ev = f4_mul(f4_add(f4_add(f4_add(Pv, Pe), Fh), Fnh2), 0.25f);
+        const float4 Eu = f4_mul(f4_add(f4_add(f4_add(Pu, Pe), Fh2), Fnh), 0.25f);
+        const float4 Ef = f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f);
+        const float4 Ef2 = f4_mul(f4_add(f4_add(f4_add(Pf2, Pe), Fnh2), Fh2), 0.25f);
+        const bool ff = fh < fh2;
+        const int64_t base = (int64_t)d.V + d.N1 + 4 * (int64_t)e;
+        st4_cs(R, base + 0, Ev);
+        st4_cs(R, base + 1, Eu);
+        st4_cs(R, base + 2, ff ? Ef : Ef2);
+        st4_cs(R, base + 3, ff ? Ef2 : Ef);
+    }
+    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e;
+}
+
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
@@ -130,7 +192,7 @@ __global__ void __launch_bounds__(BS) k_g1(FastDims d, Faces<PQ> pf, const int* 
     const float4 c2 = valid ? ldg4(P, Q.z) : f4_zero();
     const float4 c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
-    if (valid && (LAK || STATE)) tw1x = __ldg(p.tw + x);
+    if (valid && (LAK || STATE || PQ)) tw1x = __ldg(p.tw + x);
     if (valid) s1 = __ldg(p.slot + x);
     if (valid && !LAK) t1x = __ldg(p.t + x);
     const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
@@ -260,6 +322,29 @@ __global__ void __launch_bounds__(BS) k_g1(FastDims d, Faces<PQ> pf, const int* 
             write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, qnext(tw1x), qnext(tw1_px), s1, t1x, eidp_x, eidp_px);
             if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
         }
+
+        // P's edge through x, on the lane of its min->max half-edge: what k_g2
+        // does for polygon parents.  Quads h2 = tw(x) and next(h2) of the twin
+        // face are {u, ve, fh2, e_in(h2)} and {v, e_out(next h2), fh2, ve}, so
+        // their face points are rebuilt from three gathered positions.
+        const int u = __shfl_sync(0xffffffffu, Q.x, ln);
+        const float4 Pu = shfl4(c0, ln), Fnh = shfl4(fp, ln);
+        if (valid && Q.x < u) {
+            const int h2 = tw1x, nh2 = qnext(h2);
+            const int4 Q2 = __ldg(reinterpret_cast<const int4*>(ids) + h2);
+            const int eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1);
+            const float4 Pf2 = ldg4(P, Q2.z), Pi2 = ldg4(P, Q2.w), Po3 = ldg4(P, eo3);
+            float4 Fh2, Fnh2;
+            if (!LAK) {
+                Fh2 = f4_mul(f4_add(f4_add(Pu, Pf2), f4_add(c1, Pi2)), 0.25f);
+                Fnh2 = f4_mul(f4_add(f4_add(c0, Pf2), f4_add(Po3, c1)), 0.25f);
+            } else {
+                Fh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), Pu), c1), Pf2), Pi2), 4.0f);
+                Fnh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), Po3), Pf2), c1), 4.0f);
+            }
+            edge_point_vertex<LAK, STATE>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, Q2.z, c0, Pu, c1, c2, Pf2, fp, Fnh,
+                                          Fh2, Fnh2);
+        }
     }
 }
 
@@ -366,7 +451,8 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
 }
 
 // ---------------------------------------------------------------------------------------------
-// G2: the edges of P, visited in corner order.  Thread x is corner x of P (=
+// G2 (polygon P; with quad P k_g1 does this work): the edges of P, visited in
+// corner order.  Thread x is corner x of P (=
 // quad x of C); the 4 corners of a face of P are 4 consecutive lanes.  Edge e
 // of P with half-edges (h, h2) = (min->max, max->min) is computed by the lane
 // x = h, so the quantities of h's face (v, u, P's face point, C's face points
@@ -401,56 +487,11 @@ __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* 
     if (!valid || Q.x >= u) return;              // not the min->max half-edge of its edge
     if (!PQ) Fnh = ldg4(FP, nh);
     const int h = x, nh2 = pf.next(h2);
-    const int ve = Q.y, e = Q.y - d.V1 - d.F1;
-    const int fh = Q.z, fh2 = d.V1 + pf.face(h2);
+    const int ve = Q.y, fh = Q.z, fh2 = d.V1 + pf.face(h2);
     const float4 Pv = ldg4(P, Q.x), Pu = ldg4(P, u);
     const float4 Pe = ldg4(P, ve), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2);
     const float4 Fh2 = ldg4(FP, h2), Fnh2 = ldg4(FP, nh2);
-    // corners of the edge point: A=4h+1 (nbr fh, face h), B=4h2+1 (fh2, h2), C=4nh+3 (u, nh), D=4nh2+3 (v, nh2)
-    const int A = 4 * h + 1, B = 4 * h2 + 1, Cc = 4 * nh + 3, D = 4 * nh2 + 3;
-    const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D);
-    float4 nb[4], fq[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        nb[r] = rA == r ? Pf : rB == r ? Pf2 : rC == r ? Pu : Pv;
-        fq[r] = rA == r ? Fh : rB == r ? Fh2 : rC == r ? Fnh : Fnh2;
-    }
-    float4 yv;
-    if (!LAK) {
-        float4 acc = f4_zero();
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc = f4_add(acc, nb[r]);
-        yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(Pe, 2.0f), 4.0f));
-#pragma unroll
-        for (int r = 0; r < 4; ++r) yv = f4_add(yv, f4_div(fq[r], 16.0f));
-    } else {
-        float4 acc = f4_zero();
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc = f4_add(acc, fq[r]);
-        // tails {v, u, fh, fh2} in ascending id: v < u < V1 <= fh, fh2
-        const bool ff = fh < fh2;
-        acc = f4_add(acc, Pv);
-        acc = f4_add(acc, Pu);
-        acc = f4_add(acc, ff ? Pf : Pf2);
-        acc = f4_add(acc, ff ? Pf2 : Pf);
-        yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(Pe, 2.0f)), 4.0f);
-    }
-    st4_cs(R, ve, yv);
-
-    if (LAK) {
-        // edges 4e + {lower end, higher end, lower face point, higher face point}; v < u
-        const float4 Ev = f4_mul(f4_add(f4_add(f4_add(Pv, Pe), Fh), Fnh2), 0.25f);
-        const float4 Eu = f4_mul(f4_add(f4_add(f4_add(Pu, Pe), Fh2), Fnh), 0.25f);
-        const float4 Ef = f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f);
-        const float4 Ef2 = f4_mul(f4_add(f4_add(f4_add(Pf2, Pe), Fnh2), Fh2), 0.25f);
-        const bool ff = fh < fh2;
-        const int64_t base = (int64_t)d.V + d.N1 + 4 * (int64_t)e;
-        st4_cs(R, base + 0, Ev);
-        st4_cs(R, base + 1, Eu);
-        st4_cs(R, base + 2, ff ? Ef : Ef2);
-        st4_cs(R, base + 3, ff ? Ef2 : Ef);
-    }
-    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e;
+    edge_point_vertex<LAK, STATE>(d, c, R, h, nh, h2, nh2, ve, fh, fh2, Pv, Pu, Pe, Pf, Pf2, Fh, Fnh, Fh2, Fnh2);
 }
 
 // ---------------------------------------------------------------------------------------------

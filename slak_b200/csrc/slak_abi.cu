@@ -325,17 +325,17 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
                                                                     reinterpret_cast<int4*>(L.o_ids), L.o_verts,
                                                                     L.slots);
     });
-    lc.after("k_g1", 1, g1b);
-    if (!PQ) {
+    lc.after("k_g1", 1, PQ ? g1b + g2b : g1b);
+    if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
         k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts);
         lc.after("k_gf");
+        with_block(L.bs[1], [&](auto b) {
+            constexpr int BS = decltype(b)::value;
+            k_g2<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
+                                                                        L.out_state, L.o_verts);
+        });
+        lc.after("k_g2", 1, g2b);
     }
-    with_block(L.bs[1], [&](auto b) {
-        constexpr int BS = decltype(b)::value;
-        k_g2<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
-                                                                    L.o_verts);
-    });
-    lc.after("k_g2", 1, g2b);
     with_block(L.bs[2], [&](auto b) {
         constexpr int BS = decltype(b)::value;
         k_g3<LAK, STATE, BS><<<grid_for(Pl.V + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
@@ -775,6 +775,7 @@ int plan_autotune(slak_plan* p, cudaStream_t str)
     for (int li : todo) {
         Level& L = p->lv[li];
         for (int k = 0; k < 3 && rc == SLAK_OK; ++k) {
+            if (k == 1 && p->lv[li - 1].quad) continue;    // k_g2 runs for polygon parents only
             for (int ci = 0; ci < 3 && rc == SLAK_OK; ++ci) {
                 L.bs[k] = kTuneBlocks[ci];
                 float t[3] = {0.f, 0.f, 0.f};
