@@ -173,7 +173,7 @@ __device__ __forceinline__ void edge_point_vertex(const FastDims& d, QState& c, 
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
 template <bool LAK, bool STATE, bool PQ, int BS>
-__global__ void __launch_bounds__(BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+__global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
