@@ -330,10 +330,10 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         const int u = __shfl_sync(0xffffffffu, Q.x, ln);
         const float4 Pu = shfl4(c0, ln), Fnh = shfl4(fp, ln);
         if (valid && Q.x < u) {
-            const int h2 = tw1x, nh2 = qnext(h2);
-            const int4 Q2 = __ldg(reinterpret_cast<const int4*>(ids) + h2);
-            const int eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1);
-            const float4 Pf2 = ldg4(P, Q2.z), Pi2 = ldg4(P, Q2.w), Po3 = ldg4(P, eo3);
+            const int h2 = tw1x, nh2 = qnext(h2), fh2 = d.V1 + (h2 >> 2);
+            const float4 Pf2 = ldg4(P, fh2);
+            const int ei2 = __ldg(ids + 4 * (int64_t)h2 + 3), eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1);
+            const float4 Pi2 = ldg4(P, ei2), Po3 = ldg4(P, eo3);
             float4 Fh2, Fnh2;
             if (!LAK) {
                 Fh2 = f4_mul(f4_add(f4_add(Pu, Pf2), f4_add(c1, Pi2)), 0.25f);
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
                 Fh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), Pu), c1), Pf2), Pi2), 4.0f);
                 Fnh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), Po3), Pf2), c1), 4.0f);
             }
-            edge_point_vertex<LAK, STATE>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, Q2.z, c0, Pu, c1, c2, Pf2, fp, Fnh,
+            edge_point_vertex<LAK, STATE>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, fh2, c0, Pu, c1, c2, Pf2, fp, Fnh,
                                           Fh2, Fnh2);
         }
     }
