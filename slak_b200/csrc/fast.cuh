@@ -177,7 +177,11 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
-    __shared__ int4 sq[4 * BS];
+    // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores (consecutive
+    // t) and the run-order reads (4 k's of a t, then the next t) are both free
+    // of bank conflicts
+    constexpr int SQ = BS + 2;
+    __shared__ int4 sq[4 * SQ];
     const int x0 = blockIdx.x * blockDim.x;
     const int x = x0 + threadIdx.x;
     const bool valid = x < d.N1;
@@ -241,10 +245,10 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     }
     // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}: staged, then one coalesced run
     const int fpid = d.V + x;
-    sq[4 * threadIdx.x + 0] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
-    sq[4 * threadIdx.x + 1] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
-    sq[4 * threadIdx.x + 2] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
-    sq[4 * threadIdx.x + 3] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
+    sq[0 * SQ + threadIdx.x] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
+    sq[1 * SQ + threadIdx.x] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
+    sq[2 * SQ + threadIdx.x] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
+    sq[3 * SQ + threadIdx.x] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
     __syncthreads();
     {
         const int nq = min(BS, d.N1 - x0);
@@ -252,7 +256,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int j = i * BS + threadIdx.x;
-            if (j < 4 * nq) __stcs(dst + j, sq[j]);
+            if (j < 4 * nq) __stcs(dst + j, sq[(j & 3) * SQ + (j >> 2)]);
         }
     }
     if (valid) {
