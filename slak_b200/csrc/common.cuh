@@ -104,6 +104,50 @@ __device__ __forceinline__ float4 vp_finish(float4 sh, float4 sl, float4 p, int 
                        vp_finish1(sh.z, sl.z, p.z, n), vp_finish1(sh.w, sl.w, p.w, n));
 }
 
+// ---------------------------------------------------------------- in-order sums
+// add(load(k)) for k = 0..n-1, in that order, with eight loads in flight: a
+// long column's records come from L2, and a loop that waited for each one
+// would pay the full latency per slot.
+template <class Load, class Add>
+__device__ __forceinline__ void for_each_loaded(int n, Load load, Add add)
+{
+    for (int k0 = 0; k0 < n; k0 += 8) {
+        float4 t[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (k0 + i < n) t[i] = load(k0 + i);
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (k0 + i < n) add(k0 + i, t[i]);
+    }
+}
+
+// ---------------------------------------------------------------- ordering
+// The slots k = 0..n-1 of key[b..b+n) in ascending key order (equal keys by
+// slot): perm[r] = the slot of rank r.  n^2 independent compares, instead of
+// n selection passes that each wait for the previous minimum; for columns of
+// up to kRankMax slots (high-valence vertices; shorter ones stay in registers).
+constexpr int kRankMax = 64;
+__device__ __forceinline__ void rank_order(const int* __restrict__ key, int b, int n, int* perm)
+{
+    for (int k = 0; k < n; ++k) {
+        const int x = __ldg(key + b + k);
+        int r = 0, j = 0;
+        for (; j + 8 <= n; j += 8) {          // eight loads in flight before the compares
+            int y[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) y[i] = __ldg(key + b + j + i);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) r += (y[i] < x) | ((y[i] == x) & (j + i < k));
+        }
+        for (; j < n; ++j) {
+            const int y = __ldg(key + b + j);
+            r += (y < x) | ((y == x) & (j < k));
+        }
+        perm[r] = k;
+    }
+}
+
 // ---------------------------------------------------------------- status
 // Device-side status written by kernels; the host reads it after a sync.
 struct DevStatus {

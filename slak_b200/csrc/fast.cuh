@@ -571,45 +571,50 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         return;
     }
     const bool comp = compensated && n > 4;
+    const auto zf = [&](int k) { return __ldg(Z + 2 * (int64_t)(b + k)); };        // FP(x) of slot b+k
+    const auto zn = [&](int k) { return __ldg(Z + 2 * (int64_t)(b + k) + 1); };    // its neighbour
     if (!LAK) {
         if (!comp) {
             float4 acc = f4_zero();
-            for (int s = b; s < e; ++s) acc = f4_add(acc, __ldg(Z + 2 * (int64_t)s + 1));
+            for_each_loaded(n, zn, [&](int, float4 t) { acc = f4_add(acc, t); });
             yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
-            for (int s = b; s < e; ++s) yv = f4_add(yv, f4_div(__ldg(Z + 2 * (int64_t)s), nn));
+            for_each_loaded(n, zf, [&](int, float4 t) { yv = f4_add(yv, f4_div(t, nn)); });
         } else {
             float4 sh = f4_zero(), sl = f4_zero();
-            for (int s = b; s < e; ++s) dd_acc(sh, sl, __ldg(Z + 2 * (int64_t)s + 1));
-            for (int s = b; s < e; ++s) dd_acc(sh, sl, __ldg(Z + 2 * (int64_t)s));
+            for_each_loaded(n, zn, [&](int, float4 t) { dd_acc(sh, sl, t); });
+            for_each_loaded(n, zf, [&](int, float4 t) { dd_acc(sh, sl, t); });
             yv = vp_finish(sh, sl, Pv, n);
         }
         // edge points of C's edges {v, e_out(x)}, ids b..e-1:
         // 0 + (p_v + FP(x))/4 + (Z[2s+1] + Z[2 rot[s]])/4
         const int64_t EPb = (int64_t)d.V + d.N1;
-        for (int s = b; s < e; ++s) {
-            const float4 ta = f4_mul(f4_add(Pv, __ldg(Z + 2 * (int64_t)s)), 0.25f);
-            const float4 tb = f4_mul(f4_add(__ldg(Z + 2 * (int64_t)s + 1), __ldg(Z + 2 * (int64_t)__ldg(z.rot + s))),
-                                     0.25f);
-            st4_cs(R, EPb + s, f4_add(f4_add(f4_zero(), ta), tb));
-        }
+        for_each_loaded(n, [&](int k) { return f4_add(zn(k), __ldg(Z + 2 * (int64_t)__ldg(z.rot + b + k))); },
+                        [&](int k, float4 t) {
+                            const float4 ta = f4_mul(f4_add(Pv, zf(k)), 0.25f);
+                            st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), ta), f4_mul(t, 0.25f)));
+                        });
     } else {
         // face points in column order, then the tails e_in(x) in ascending id
         float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
-        for (int s = b; s < e; ++s) {
-            const float4 f = __ldg(Z + 2 * (int64_t)s);
-            if (comp) dd_acc(sh, sl, f); else acc = f4_add(acc, f);
-        }
-        int last = -1;
-        while (true) {
-            int xm = INT32_MAX, sm = -1;
-            for (int s = b; s < e; ++s) {
-                const int ti = __ldg(z.T + s);
-                if (ti > last && ti < xm) { xm = ti; sm = s; }
+        for_each_loaded(n, zf, [&](int, float4 t) { if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t); });
+        if (n <= kRankMax) {
+            int perm[kRankMax];
+            rank_order(z.T, b, n, perm);
+            for_each_loaded(n, [&](int r) { return zn(perm[r]); },
+                            [&](int, float4 t) { if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t); });
+        } else {
+            int last = -1;
+            while (true) {
+                int xm = INT32_MAX, sm = -1;
+                for (int s = b; s < e; ++s) {
+                    const int ti = __ldg(z.T + s);
+                    if (ti > last && ti < xm) { xm = ti; sm = s; }
+                }
+                if (sm < 0) break;
+                const float4 pt = __ldg(Z + 2 * (int64_t)sm + 1);
+                if (comp) dd_acc(sh, sl, pt); else acc = f4_add(acc, pt);
+                last = xm;
             }
-            if (sm < 0) break;
-            const float4 pt = __ldg(Z + 2 * (int64_t)sm + 1);
-            if (comp) dd_acc(sh, sl, pt); else acc = f4_add(acc, pt);
-            last = xm;
         }
         if (comp) yv = vp_finish(sh, sl, Pv, n);
         else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);

@@ -281,8 +281,18 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
     const int b = sptr[v], e = sptr[v + 1];
     int id = eptr[v], last = -1;
     while (true) {
-        int x = INT32_MAX;
-        for (int s = b; s < e; ++s) {
+        int x = INT32_MAX, s = b;
+        for (; s + 4 <= e; s += 4) {          // the column's loads issued four slots at a time
+            int w[4], u[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { w[i] = __ldg(snext + s + i); u[i] = __ldg(sprev + s + i); }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (w[i] > last && w[i] < v && w[i] < x) x = w[i];
+                if (u[i] > last && u[i] < v && u[i] < x) x = u[i];
+            }
+        }
+        for (; s < e; ++s) {
             int w = snext[s], u = sprev[s];
             if (w > last && w < v && w < x) x = w;
             if (u > last && u < v && u < x) x = u;
@@ -398,19 +408,21 @@ __global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, c
     const int b = sptr[v], e = sptr[v + 1], n = e - b;
     const float nn = (float)(n * n);
     float4 y;
+    const auto nbr = [&](int k) { return ldg4(P, __ldg(snext + b + k)); };
+    const auto fpt = [&](int k) { return ldg4(FP, fc.face(__ldg(sc + b + k))); };
     if (!compensated || n <= 4) {
         float4 acc = f4_zero();
-        for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(P, snext[s]));
+        for_each_loaded(n, nbr, [&](int, float4 t) { acc = f4_add(acc, t); });
         float4 orig = f4_div(f4_mul(ldg4(P, v), (float)(n - 2)), (float)n);
         y = f4_add(f4_div(acc, nn), orig);
-        for (int s = b; s < e; ++s) y = f4_add(y, f4_div(ldg4(FP, fc.face(sc[s])), nn));
+        for_each_loaded(n, fpt, [&](int, float4 t) { y = f4_add(y, f4_div(t, nn)); });
     } else {
         // compensated: the 2n neighbour and face terms are summed as an unevaluated
         // float pair (TwoSum), divided by n^2 with an exact remainder, and added to
         // p (n-2)/n evaluated the same way; one rounding at the end
         float4 sh = f4_zero(), sl = f4_zero();
-        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(P, snext[s]));
-        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, fc.face(sc[s])));
+        for_each_loaded(n, nbr, [&](int, float4 t) { dd_acc(sh, sl, t); });
+        for_each_loaded(n, fpt, [&](int, float4 t) { dd_acc(sh, sl, t); });
         y = vp_finish(sh, sl, ldg4(P, v), n);
     }
     if (boundary) {
@@ -442,15 +454,25 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    const auto fpt = [&](int k) { return ldg4(FP, fc.face(__ldg(sc + b + k))); };
     float4 acc = f4_zero();
-    for (int s = b; s < e; ++s) acc = f4_add(acc, ldg4(FP, fc.face(sc[s])));
-    int last = -1;
-    while (true) {
-        int x = INT32_MAX;
-        for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > last && u < x) x = u; }
-        if (x == INT32_MAX) break;
-        acc = f4_add(acc, ldg4(P, x));
-        last = x;
+    for_each_loaded(n, fpt, [&](int, float4 t) { acc = f4_add(acc, t); });
+    // the tails (distinct neighbours) in ascending id
+    int perm[kRankMax];
+    const bool ranked = n <= kRankMax;
+    if (ranked) rank_order(sprev, b, n, perm);
+    const auto tail = [&](int r) { return ldg4(P, __ldg(sprev + b + perm[r])); };
+    if (ranked) {
+        for_each_loaded(n, tail, [&](int, float4 t) { acc = f4_add(acc, t); });
+    } else {
+        int last = -1;
+        while (true) {
+            int x = INT32_MAX;
+            for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > last && u < x) x = u; }
+            if (x == INT32_MAX) break;
+            acc = f4_add(acc, ldg4(P, x));
+            last = x;
+        }
     }
     float4 y;
     if (!compensated || n <= 4) {
@@ -459,13 +481,17 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
     } else {
         // same terms, summed with TwoSum and finished with exact remainders
         float4 sh = f4_zero(), sl = f4_zero();
-        for (int s = b; s < e; ++s) dd_acc(sh, sl, ldg4(FP, fc.face(sc[s])));
-        for (int l2 = -1;;) {
-            int x = INT32_MAX;
-            for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > l2 && u < x) x = u; }
-            if (x == INT32_MAX) break;
-            dd_acc(sh, sl, ldg4(P, x));
-            l2 = x;
+        for_each_loaded(n, fpt, [&](int, float4 t) { dd_acc(sh, sl, t); });
+        if (ranked) {
+            for_each_loaded(n, tail, [&](int, float4 t) { dd_acc(sh, sl, t); });
+        } else {
+            for (int l2 = -1;;) {
+                int x = INT32_MAX;
+                for (int s = b; s < e; ++s) { int u = sprev[s]; if (u > l2 && u < x) x = u; }
+                if (x == INT32_MAX) break;
+                dd_acc(sh, sl, ldg4(P, x));
+                l2 = x;
+            }
         }
         y = vp_finish(sh, sl, ldg4(P, v), n);
     }
