@@ -186,6 +186,7 @@ def run_ours(args, dist, rank, ws):
         _barrier(dist)
         st = plan.check(stream)
     ms = [a.elapsed_time(b) for a, b in ev]
+    spread = {"min": min(ms), "median": statistics.median(ms), "max": max(ms)}
     ms_step = _max_over_ranks(dist, statistics.mean(ms))
     value = faces * ws / (ms_step * 1e-3)
     launches = plan.launches * args.steps
@@ -224,6 +225,7 @@ def run_ours(args, dist, rank, ws):
                    "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
                    "parallelism": f"replicas x{ws}"},
         "gpu_launches": launches,
+        "ms_per_step_spread": spread,
         "roofline": kern,
         "kernels": ktable[:8],
         "levels": per_level,
@@ -513,6 +515,7 @@ def run_reference(args, dist, rank, ws):
     faces = sizes[-1][2]
     ms_step = statistics.mean(ms)
     value = faces / (ms_step * 1e-3)
+    spread = {"min": min(ms), "median": statistics.median(ms), "max": max(ms)}
     # end to end through the reference's public call with host buffers: the
     # same pinned H2D of the input and D2H of the refined ids and positions as
     # this repository's e2e figure
@@ -527,6 +530,7 @@ def run_reference(args, dist, rank, ws):
                                f"{faces} quads", "scheme": args.scheme.upper(), "levels": levels,
                    "refined_faces": faces, "parallelism": "replicas x1"},
         "reference_self_reported_ms": statistics.mean(self_ms) if self_ms else None,
+        "ms_per_step_spread": spread,
         "cpu_baseline": {"value": value, "unit": "refined_faces/s", "cores": 1, "kind": "reference",
                          "sample": "GPUPeople/SLAK's own CUDA path (built for sm_100a) on the full workload; "
                                    "the reference has no CPU implementation"},
