@@ -105,19 +105,19 @@ __device__ __forceinline__ float4 vp_finish(float4 sh, float4 sl, float4 p, int 
 }
 
 // ---------------------------------------------------------------- in-order sums
-// add(load(k)) for k = 0..n-1, in that order, with eight loads in flight: a
+// add(load(k)) for k = 0..n-1, in that order, with W loads in flight: a
 // long column's records come from L2, and a loop that waited for each one
 // would pay the full latency per slot.
-template <class Load, class Add>
+template <int W = 4, class Load, class Add>
 __device__ __forceinline__ void for_each_loaded(int n, Load load, Add add)
 {
-    for (int k0 = 0; k0 < n; k0 += 8) {
-        float4 t[8];
+    for (int k0 = 0; k0 < n; k0 += W) {
+        float4 t[W];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < W; ++i)
             if (k0 + i < n) t[i] = load(k0 + i);
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < W; ++i)
             if (k0 + i < n) add(k0 + i, t[i]);
     }
 }
