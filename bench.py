@@ -38,7 +38,7 @@ HBM_FALLBACK_GBS = 6650.0
 # kernel, from one ncu capture of a smaller case of the same structure
 # (profiles/k_g_fast_levels_mixed384_slak.txt: k_g1 of the last level, SLAK,
 # per quad of the level it refines); scaled by the units of the bench's launch.
-TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 169.76}
+TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 183.03}
 
 
 def _peaks():
