@@ -194,7 +194,11 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     const float4 c0 = valid ? ldg4(P, Q.x) : f4_zero();
     const float4 c1 = valid ? ldg4(P, Q.y) : f4_zero();
     const float4 c2 = valid ? ldg4(P, Q.z) : f4_zero();
-    const float4 c3 = valid ? ldg4(P, Q.w) : f4_zero();
+    // with quad P, e_in(x) is e_out(prev x): the previous lane's c1 (a shuffle
+    // instead of a fourth scattered gather)
+    float4 c3;
+    if constexpr (PQ) c3 = shfl4(c1, (threadIdx.x & 31 & ~3) | ((x + 3) & 3));
+    else c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
     if (valid && (LAK || STATE || PQ)) tw1x = __ldg(p.tw + x);
     if (valid) s1 = __ldg(p.slot + x);
