@@ -90,6 +90,25 @@ const char* slak_last_error_detail(void);
 int slak_subdivide(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
                    slak_stream_t stream);
 
+/*
+ * Mesh files (host memory).  slak_obj_read replaces OBJ::read + the
+ * GPU::CSCMesh(path) constructor (include/obj.h:107-257,
+ * include/Mesh.h:153-176): it fills *out with host arrays (malloc) in the
+ * MeshInfo layout -- face offsets ptr (F+1), 0-based corner ids (N), vals =
+ * each corner's 1-based position in its face, verts = (x, y, z, 1) -- and the
+ * type TRI / QUAD / POLY from the face sizes.  "v" and "f" lines are read
+ * ("f" corners as v, v/vt, v//vn or v/vt/vn; negative indices count back from
+ * the vertices read so far); other lines are skipped.  A face with fewer than
+ * three corners or an index out of range gives SLAK_ERR_BAD_MESH.  The file is
+ * parsed by several threads.  Release with slak_obj_free.
+ * slak_obj_write replaces OBJ::write (include/obj.h:259-297) for a host mesh:
+ * "v x y z" lines (9 significant digits, so float32 positions read back
+ * exactly) and 1-based "f" lines (QUAD / TRI faces need no ptr).
+ */
+int slak_obj_read(const char* path, slak_mesh* out);
+int slak_obj_write(const char* path, const slak_mesh* host_mesh);
+int slak_obj_free(slak_mesh* host_mesh);
+
 /* Frees the current device's cached slak_subdivide workspace.  No counterpart
  * in the reference, whose calls keep nothing between them.  Returns
  * SLAK_ERR_NOT_READY while a call holds the workspace. */

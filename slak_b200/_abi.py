@@ -18,7 +18,8 @@ PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4
 
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
-           "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_plan_create",
+           "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_obj_read", "slak_obj_write",
+           "slak_obj_free", "slak_plan_create",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
@@ -78,6 +79,11 @@ def lib():
         L.slak_last_error_detail.restype = ctypes.c_char_p
         L.slak_subdivide.argtypes = [P, P, I, I, V]
         L.slak_mesh_free.argtypes = [P]
+        L.slak_obj_read.argtypes = [ctypes.c_char_p, P]
+        L.slak_obj_write.argtypes = [ctypes.c_char_p, P]
+        L.slak_obj_free.argtypes = [P]
+        for n in ("slak_obj_read", "slak_obj_write", "slak_obj_free"):
+            getattr(L, n).restype = I
         L.slak_workspace_release.argtypes = []
         L.slak_workspace_release.restype = I
         L.slak_subdivide_level_noalloc.argtypes = [P, P, I, V]

@@ -50,7 +50,7 @@ def _csrc(*names):
 
 def build_cuda(verbose=False, force=False, extra=None):
     os.makedirs(_paths.LIB_DIR, exist_ok=True)
-    srcs = _csrc("slak_abi.cu")
+    srcs = _csrc("slak_abi.cu") + _csrc("objio.cpp")
     deps = srcs + [os.path.join(_paths.CSRC_DIR, f) for f in os.listdir(_paths.CSRC_DIR)
                    if f.endswith((".cuh", ".h"))] + [os.path.join(_paths.INCLUDE_DIR, "slak_b200.h")]
     if not force and not _stale(_paths.LIB_SLAK, deps):

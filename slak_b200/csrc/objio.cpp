@@ -1,0 +1,278 @@
+// objio.cpp -- Wavefront OBJ reading and writing on the host, in parallel.
+//
+// The reference reads meshes with OBJ::read (include/obj.h:107-257) into
+// GPU::CSCMesh (include/Mesh.h:153-176): face offsets, 0-based corner vertex
+// indices (negative OBJ indices count back from the vertices read so far),
+// vals = the corner's 1-based position in its face, positions (x, y, z, 1),
+// type TRI / QUAD / POLY from the face sizes.  This file produces the same
+// arrays.  The file is split into newline-aligned chunks parsed by one thread
+// each: a first pass counts each chunk's "v" lines, so a chunk knows how many
+// vertices precede it and can resolve negative indices; a second pass parses.
+// Writing formats chunks of lines in parallel and writes them in order.
+#include "slak_b200.h"
+
+#include <algorithm>
+#include <cerrno>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+struct Chunk {
+    const char* b;
+    const char* e;
+    int64_t nv = 0;            // "v" lines in the chunk (first pass)
+    std::vector<float> v;      // x, y, z per vertex
+    std::vector<int32_t> fo;   // face sizes
+    std::vector<int32_t> fi;   // corner vertex indices, 0-based
+    int err_line = 0;          // nonzero: 1-based line (within the chunk) of a malformed face
+    int64_t lines = 0;
+};
+
+inline const char* skip_ws(const char* p, const char* e)
+{
+    while (p < e && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+    return p;
+}
+
+inline const char* line_end(const char* p, const char* e)
+{
+    const void* q = std::memchr(p, '\n', (size_t)(e - p));
+    return q ? static_cast<const char*>(q) : e;
+}
+
+inline bool is_v(const char* p, const char* le) { return le - p >= 2 && p[0] == 'v' && (p[1] == ' ' || p[1] == '\t'); }
+inline bool is_f(const char* p, const char* le) { return le - p >= 2 && p[0] == 'f' && (p[1] == ' ' || p[1] == '\t'); }
+
+void count_pass(Chunk& c)
+{
+    for (const char* p = c.b; p < c.e;) {
+        const char* le = line_end(p, c.e);
+        const char* s = skip_ws(p, le);
+        if (is_v(s, le)) ++c.nv;
+        p = le + 1;
+    }
+}
+
+// base: vertices defined before this chunk
+void parse_pass(Chunk& c, int64_t base)
+{
+    int64_t nv = base;
+    std::string tmp;
+    for (const char* p = c.b; p < c.e;) {
+        const char* le = line_end(p, c.e);
+        ++c.lines;
+        const char* s = skip_ws(p, le);
+        if (is_v(s, le)) {
+            tmp.assign(s + 2, le);
+            char* q = &tmp[0];
+            char* end = nullptr;
+            for (int k = 0; k < 3; ++k) {
+                float x = std::strtof(q, &end);
+                if (end == q) x = 0.f;
+                c.v.push_back(x);
+                q = end;
+            }
+            ++nv;
+        } else if (is_f(s, le)) {
+            int32_t order = 0;
+            const char* q = s + 2;
+            while (true) {
+                q = skip_ws(q, le);
+                if (q >= le) break;
+                // one corner: v, v/vt, v//vn or v/vt/vn; only v is kept
+                char* end = nullptr;
+                long vi = std::strtol(q, &end, 10);
+                if (end == q) { c.err_line = (int)c.lines; break; }
+                const int64_t idx = vi < 0 ? nv + vi : (int64_t)vi - 1;
+                if (vi == 0 || idx < 0) { c.err_line = (int)c.lines; break; }
+                c.fi.push_back((int32_t)idx);
+                ++order;
+                q = end;
+                while (q < le && *q != ' ' && *q != '\t' && *q != '\r') ++q;
+            }
+            if (c.err_line) break;
+            c.fo.push_back(order);
+        }
+        p = le + 1;
+    }
+}
+
+int nthreads_for(size_t bytes)
+{
+    unsigned hc = std::thread::hardware_concurrency();
+    const size_t by_size = bytes / (size_t(1) << 20) + 1;     // about 1 MB per thread at least
+    return (int)std::max<size_t>(1, std::min<size_t>(hc ? hc : 1, by_size));
+}
+
+}  // namespace
+
+extern "C" {
+
+int slak_obj_read(const char* path, slak_mesh* out)
+{
+    if (!path || !out) return SLAK_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof(*out));
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SLAK_ERR_INVALID_ARG;
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    std::vector<char> buf((size_t)std::max(size, 0L));
+    const size_t got = size > 0 ? std::fread(buf.data(), 1, buf.size(), f) : 0;
+    std::fclose(f);
+    if (got != buf.size()) return SLAK_ERR_INVALID_ARG;
+    const char* b = buf.data();
+    const char* e = b + buf.size();
+
+    const int nt = nthreads_for(buf.size());
+    std::vector<Chunk> ch(nt);
+    for (int t = 0; t < nt; ++t) {
+        // chunk t ends after the line holding its nominal end point
+        const char* cb = t == 0 ? b : ch[t - 1].e;
+        const char* ce = t + 1 == nt ? e : b + buf.size() * (size_t)(t + 1) / (size_t)nt;
+        if (ce < cb) ce = cb;
+        if (ce < e) {
+            const char* q = line_end(ce, e);
+            ce = q < e ? q + 1 : e;
+        }
+        ch[t].b = cb;
+        ch[t].e = ce;
+    }
+    auto run = [&](auto fn) {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; ++t) th.emplace_back(fn, t);
+        fn(0);
+        for (auto& x : th) x.join();
+    };
+    run([&](int t) { count_pass(ch[t]); });
+    std::vector<int64_t> vbase(nt + 1, 0);
+    for (int t = 0; t < nt; ++t) vbase[t + 1] = vbase[t] + ch[t].nv;
+    run([&](int t) { parse_pass(ch[t], vbase[t]); });
+
+    int64_t F = 0, N = 0, V = vbase[nt];
+    for (auto& c : ch) {
+        if (c.err_line) return SLAK_ERR_BAD_MESH;
+        F += (int64_t)c.fo.size();
+        N += (int64_t)c.fi.size();
+    }
+    if (N >= (int64_t(1) << 31) || V >= (int64_t(1) << 31)) return SLAK_ERR_UNSUPPORTED;
+    int32_t* ptr = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)(F + 1)));
+    int32_t* ids = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(N, 1)));
+    int32_t* vals = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)std::max<int64_t>(N, 1)));
+    float* verts = static_cast<float*>(std::malloc(sizeof(float) * 4 * (size_t)std::max<int64_t>(V, 1)));
+    if (!ptr || !ids || !vals || !verts) {
+        std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
+        return SLAK_ERR_OOM;
+    }
+    std::vector<int64_t> fbase(nt + 1, 0), nbase(nt + 1, 0);
+    for (int t = 0; t < nt; ++t) {
+        fbase[t + 1] = fbase[t] + (int64_t)ch[t].fo.size();
+        nbase[t + 1] = nbase[t] + (int64_t)ch[t].fi.size();
+    }
+    int min_order = INT32_MAX, max_order = 0;
+    for (auto& c : ch)
+        for (int32_t o : c.fo) { min_order = std::min(min_order, (int)o); max_order = std::max(max_order, (int)o); }
+    bool bad = F > 0 && min_order < 3;
+    run([&](int t) {
+        const Chunk& c = ch[t];
+        int64_t off = nbase[t];
+        for (size_t k = 0; k < c.fo.size(); ++k) {
+            ptr[fbase[t] + (int64_t)k] = (int32_t)off;
+            for (int32_t j = 0; j < c.fo[k]; ++j) vals[off + j] = j + 1;
+            off += c.fo[k];
+        }
+        std::memcpy(ids + nbase[t], c.fi.data(), sizeof(int32_t) * c.fi.size());
+        for (int64_t k = 0; k < c.nv; ++k) {
+            float* o = verts + 4 * (vbase[t] + k);
+            o[0] = c.v[3 * k]; o[1] = c.v[3 * k + 1]; o[2] = c.v[3 * k + 2]; o[3] = 1.0f;
+        }
+    });
+    ptr[F] = (int32_t)N;
+    for (int64_t c = 0; c < N && !bad; ++c) bad = ids[c] >= V;
+    if (bad) {
+        std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
+        return SLAK_ERR_BAD_MESH;
+    }
+    out->type = (F > 0 && min_order == 3 && max_order == 3) ? SLAK_MESH_TRI
+              : (F > 0 && min_order == 4 && max_order == 4) ? SLAK_MESH_QUAD : SLAK_MESH_POLY;
+    out->is_reduced = 1;
+    out->nfaces = F;
+    out->nverts = V;
+    out->nnz = N;
+    out->max_face_order = max_order;
+    out->ptr = ptr;
+    out->ids = ids;
+    out->vals = vals;
+    out->verts = verts;
+    return SLAK_OK;
+}
+
+int slak_obj_write(const char* path, const slak_mesh* m)
+{
+    if (!path || !m || m->nverts < 0 || m->nfaces < 0 || (m->nverts > 0 && !m->verts)) return SLAK_ERR_INVALID_ARG;
+    const int fixed = m->type == SLAK_MESH_QUAD ? 4 : m->type == SLAK_MESH_TRI ? 3 : 0;
+    if (m->nfaces > 0 && (!m->ids || (!fixed && !m->ptr))) return SLAK_ERR_INVALID_ARG;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return SLAK_ERR_INVALID_ARG;
+    const int64_t V = m->nverts, F = m->nfaces;
+    const int nt = nthreads_for((size_t)(V + F) * 32);
+    std::vector<std::string> part(nt);
+    // vertices, then faces; each thread formats a contiguous range of lines
+    auto fmt_range = [&](int t) {
+        std::string& s = part[t];
+        char line[160];
+        const int64_t vb = V * t / nt, ve = V * (t + 1) / nt;
+        for (int64_t i = vb; i < ve; ++i) {
+            const float* p = m->verts + 4 * i;
+            const int n = std::snprintf(line, sizeof line, "v %.9g %.9g %.9g\n", p[0], p[1], p[2]);
+            s.append(line, (size_t)n);
+        }
+    };
+    std::vector<std::string> fpart(nt);
+    auto fmt_faces = [&](int t) {
+        std::string& s = fpart[t];
+        char num[16];
+        const int64_t fb = F * t / nt, fe = F * (t + 1) / nt;
+        for (int64_t g = fb; g < fe; ++g) {
+            const int64_t b = fixed ? g * fixed : m->ptr[g];
+            const int64_t e = fixed ? b + fixed : m->ptr[g + 1];
+            s.push_back('f');
+            for (int64_t c = b; c < e; ++c) {
+                const int n = std::snprintf(num, sizeof num, " %d", m->ids[c] + 1);
+                s.append(num, (size_t)n);
+            }
+            s.push_back('\n');
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; ++t) th.emplace_back([&, t] { fmt_range(t); fmt_faces(t); });
+        fmt_range(0);
+        fmt_faces(0);
+        for (auto& x : th) x.join();
+    }
+    bool ok = true;
+    for (auto& s : part) ok &= std::fwrite(s.data(), 1, s.size(), f) == s.size();
+    for (auto& s : fpart) ok &= std::fwrite(s.data(), 1, s.size(), f) == s.size();
+    ok &= std::fclose(f) == 0;
+    return ok ? SLAK_OK : SLAK_ERR_INVALID_ARG;
+}
+
+int slak_obj_free(slak_mesh* m)
+{
+    if (!m) return SLAK_ERR_INVALID_ARG;
+    std::free(m->ptr);
+    std::free(m->ids);
+    std::free(m->vals);
+    std::free(m->verts);
+    std::memset(m, 0, sizeof(*m));
+    return SLAK_OK;
+}
+
+}  // extern "C"

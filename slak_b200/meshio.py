@@ -1,0 +1,52 @@
+"""Wavefront OBJ files <-> host meshes (slak_obj_read / slak_obj_write).
+
+The arrays are the reference's CSCMesh layout (include/Mesh.h:153-176):
+face offsets, 0-based corner ids, vals = 1-based corner position in its face,
+positions (x, y, z, 1); the mesh type is TRI / QUAD / POLY from the face sizes.
+The parse runs multi-threaded in the C++ library.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _abi
+from .mesh import QUAD, TRI, Mesh
+
+
+def read_obj(path: str) -> Mesh:
+    c = _abi.SlakMesh()
+    _abi.check(_abi.lib().slak_obj_read(os.fsencode(path), ctypes.byref(c)), f"slak_obj_read({path})")
+    try:
+        F, N, V = int(c.nfaces), int(c.nnz), int(c.nverts)
+        arr = lambda p, n, t: np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(t)), shape=(n,)).copy()
+        ptr = arr(c.ptr, F + 1, ctypes.c_int32)
+        ids = arr(c.ids, N, ctypes.c_int32) if N else np.zeros(0, np.int32)
+        vals = arr(c.vals, N, ctypes.c_int32) if N else np.zeros(0, np.int32)
+        verts = arr(c.verts, 4 * V, ctypes.c_float).reshape(V, 4) if V else np.zeros((0, 4), np.float32)
+        return Mesh(int(c.type), ids, verts, ptr, vals, F, int(c.max_face_order), True)
+    finally:
+        _abi.lib().slak_obj_free(ctypes.byref(c))
+
+
+def write_obj(path: str, mesh) -> None:
+    """Writes a host mesh (a Mesh, or any object with its fields, e.g. a
+    refined HostResult); QUAD and TRI meshes need no face offsets."""
+    keep = []
+
+    def p(a, dt):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    c = _abi.SlakMesh()
+    c.type = int(mesh.type)
+    c.nfaces, c.nverts, c.nnz = int(mesh.nfaces), int(mesh.nverts), int(mesh.nnz)
+    c.ptr = p(None if mesh.type in (QUAD, TRI) else mesh.ptr, np.int32)
+    c.ids = p(mesh.ids, np.int32)
+    c.verts = p(np.asarray(mesh.verts, np.float32).reshape(-1), np.float32)
+    _abi.check(_abi.lib().slak_obj_write(os.fsencode(path), ctypes.byref(c)), f"slak_obj_write({path})")
