@@ -48,13 +48,15 @@ __device__ __forceinline__ int qprev(int x) { return (x & ~3) | ((x + 3) & 3); }
 struct QState {
     int* sptr;
     int* slot;
-    int* tw;
-    int* t;
+    int* tw;       // -1: no twin (boundary half-edge)
+    int* t;        // -1: the previous corner's half-edge has no twin
+    int* brank;    // per edge: boundary edges with a smaller id (meshes with a boundary)
 };
 
 struct FastDims {
     int N1, V1, F1, E1;    // P
-    int V, N;              // C (F = N1, E = 2 N1)
+    int V, N;              // C (F = N1, E = 2 N1 + B1)
+    int B1;                // P's boundary edges (0: closed)
 };
 
 __device__ __forceinline__ float4 shfl4(float4 v, int src)
@@ -85,29 +87,41 @@ __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a
 // vertex across the edge e_in(x) = e_out(y), so half-edge 4x+3's share of SLAK
 // edge point t1(x), (P[e_in(x)] + FP(x)) / 4, is (Z[2 t1(x) + 1] + Z[2 rot]) / 4:
 // two records of the same column, which k_g3 has loaded anyway.
+// Meshes with a boundary add, per slot: bflag (bit 0: the corner's outgoing
+// half-edge has no twin, bit 1: its incoming one), bid (the boundary neighbour
+// the records lack: SLAK e_in(x), LAK e_out(x)) and bscan (bit 0 again, the
+// input of the scan that ranks C's boundary edges, SLAK).
 struct SlotScratch {
     float4* Z;
     int* T;      // LAK
     int* rot;    // SLAK (the same memory as T: one scheme per plan)
+    int* bflag;
+    int* bid;
+    int* bscan;
 };
 
-// C's slot / twin / t for its corners 4x+k (the state the next fast level reads)
+// C's slot / twin / t for its corners 4x+k (the state the next fast level
+// reads).  With a boundary, a P edge without a twin gives its edge point 2
+// corners instead of 4 (absent corners rank last), its columns start at
+// 2 N1 + 4e - 2 brank(e), and C's half-edges along it have no twin.
 template <bool LAK>
 __device__ __forceinline__ void write_state(const FastDims& d, QState& c, int x, int nxx, int px, int tw1x,
                                             int tw1_px, int ntw, int ntwp, int s1, int t1x, int eidp_x,
-                                            int eidp_px)
+                                            int eidp_px, int br_x = 0, int br_px = 0)
 {
+    const bool tx = tw1x >= 0, tpx = tw1_px >= 0;
     // edge of P through x: corners A=4x+1, B=4tw1x+1, Cc=4nxx+3, D=4ntw+3
-    const int A = 4 * x + 1, B = 4 * tw1x + 1, Cc = 4 * nxx + 3, D = 4 * ntw + 3;
+    const int A = 4 * x + 1, B = tx ? 4 * tw1x + 1 : INT32_MAX, Cc = 4 * nxx + 3, D = tx ? 4 * ntw + 3 : INT32_MAX;
     // edge of P through prev(x): A'=4px+1, B'=4tw1_px+1, C'=4x+3, D'=4ntwp+3
-    const int A2 = 4 * px + 1, B2 = 4 * tw1_px + 1, C2 = 4 * x + 3, D2 = 4 * ntwp + 3;
-    const int base_x = 2 * d.N1 + 4 * eidp_x, base_px = 2 * d.N1 + 4 * eidp_px;
-    reinterpret_cast<int4*>(c.tw)[x] = make_int4(4 * ntw + 3, 4 * nxx + 2, 4 * px + 1, 4 * tw1_px);
+    const int A2 = 4 * px + 1, B2 = tpx ? 4 * tw1_px + 1 : INT32_MAX, C2 = 4 * x + 3;
+    const int D2 = tpx ? 4 * ntwp + 3 : INT32_MAX;
+    const int base_x = 2 * d.N1 + 4 * eidp_x - 2 * br_x, base_px = 2 * d.N1 + 4 * eidp_px - 2 * br_px;
+    reinterpret_cast<int4*>(c.tw)[x] = make_int4(tx ? 4 * ntw + 3 : -1, 4 * nxx + 2, 4 * px + 1, tpx ? 4 * tw1_px : -1);
     reinterpret_cast<int4*>(c.slot)[x] =
         make_int4(s1, base_x + rank4(A, B, Cc, D), d.N1 + x, base_px + rank4(C2, A2, B2, D2));
     if (!LAK)
         reinterpret_cast<int4*>(c.t)[x] =
-            make_int4(t1x, base_x + rank4(D, A, B, Cc), d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
+            make_int4(t1x, tx ? base_x + rank4(D, A, B, Cc) : -1, d.N1 + nxx, base_px + rank4(A2, B2, C2, D2));
 }
 
 // The vertex point of P's edge point ve (edge e = ve - V1 - F1, half-edges
@@ -115,13 +129,14 @@ __device__ __forceinline__ void write_state(const FastDims& d, QState& c, int x,
 // 4e..4e+3 of C around it.  Inputs: the positions of v, u, ve and of the two
 // face points fh (of h's face), fh2 (of h2's); C's face points of quads h,
 // next(h), h2, next(h2).
-template <bool LAK, bool STATE>
+template <bool LAK, bool STATE, bool BND = false>
 __device__ __forceinline__ void edge_point_vertex(const FastDims& d, QState& c, float* __restrict__ R, int h,
                                                   int nh, int h2, int nh2, int ve, int fh, int fh2, float4 Pv,
                                                   float4 Pu, float4 Pe, float4 Pf, float4 Pf2, float4 Fh, float4 Fnh,
-                                                  float4 Fh2, float4 Fnh2)
+                                                  float4 Fh2, float4 Fnh2, int br = 0)
 {
     const int e = ve - d.V1 - d.F1;
+    const int ce = 4 * e - br;                 // LAK: C's first edge around ve (boundary P edges have 3)
     // corners of the edge point: A=4h+1 (nbr fh, face h), B=4h2+1 (fh2, h2), C=4nh+3 (u, nh), D=4nh2+3 (v, nh2)
     const int A = 4 * h + 1, B = 4 * h2 + 1, Cc = 4 * nh + 3, D = 4 * nh2 + 3;
     const int rA = rank4(A, B, Cc, D), rB = rank4(B, A, Cc, D), rC = rank4(Cc, A, B, D);
@@ -160,23 +175,61 @@ __device__ __forceinline__ void edge_point_vertex(const FastDims& d, QState& c, 
         const float4 Ef = f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f);
         const float4 Ef2 = f4_mul(f4_add(f4_add(f4_add(Pf2, Pe), Fnh2), Fh2), 0.25f);
         const bool ff = fh < fh2;
-        const int64_t base = (int64_t)d.V + d.N1 + 4 * (int64_t)e;
+        const int64_t base = (int64_t)d.V + d.N1 + ce;
         st4_cs(R, base + 0, Ev);
         st4_cs(R, base + 1, Eu);
         st4_cs(R, base + 2, ff ? Ef : Ef2);
         st4_cs(R, base + 3, ff ? Ef2 : Ef);
+        if (STATE && BND)
+            for (int k = 0; k < 4; ++k) c.brank[ce + k] = 2 * br;     // ce is not 4-aligned
     }
-    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e;
+    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e - 2 * br;
+}
+
+// A P edge without a twin (half-edge h: v -> u in the face of h): its edge
+// point ve is on C's boundary, so its vertex point is 3/4 p + 1/8 of its two
+// boundary neighbours (SLAK: u then v, correctBoundaryS2 CatmullClarkKernels.cuh
+// :709-740; LAK: ascending edge id, i.e. the lower of v, u first,
+// calculateExternalVertexUpdate LAKCatmullClarkKernels.cuh:483-511).  C's
+// boundary edges {v, ve} and {ve, u} get midpoints (correctBoundaryS1 :688-707,
+// calculateExternalEdgepoints :452-462): SLAK writes {ve, u} (id 2 N1 +
+// brank(e)) here and {v, ve} (id slot(h)) in k_g3; LAK writes C's three edges
+// around ve, ids 4e - brank(e) + {lower end, higher end, face point}.
+template <bool LAK, bool STATE>
+__device__ __forceinline__ void boundary_edge(const FastDims& d, QState& c, float* __restrict__ R, int v, int u,
+                                              int ve, int br, float4 Pv, float4 Pu, float4 Pe, float4 Pf, float4 Fh,
+                                              float4 Fnh)
+{
+    const int e = ve - d.V1 - d.F1;
+    const int64_t EP = (int64_t)d.V + d.N1;
+    if (!LAK) {
+        st4(R, ve, f4_add(f4_add(f4_mul(Pe, 0.75f), f4_mul(Pu, 0.125f)), f4_mul(Pv, 0.125f)));
+        st4_cs(R, EP + 2 * (int64_t)d.N1 + br, f4_mul(f4_add(Pe, Pu), 0.5f));
+        if (STATE) c.brank[2 * d.N1 + br] = d.B1 + br;
+    } else {
+        const bool vu = v < u;
+        const float4 Plo = vu ? Pv : Pu, Phi = vu ? Pu : Pv;
+        st4(R, ve, f4_add(f4_add(f4_mul(Pe, 0.75f), f4_mul(Plo, 0.125f)), f4_mul(Phi, 0.125f)));
+        const int ce = 4 * e - br;
+        st4_cs(R, EP + ce + 0, f4_mul(f4_add(Plo, Pe), 0.5f));
+        st4_cs(R, EP + ce + 1, f4_mul(f4_add(Phi, Pe), 0.5f));
+        st4_cs(R, EP + ce + 2, f4_mul(f4_add(f4_add(f4_add(Pf, Pe), Fnh), Fh), 0.25f));
+        if (STATE) { c.brank[ce] = 2 * br; c.brank[ce + 1] = 2 * br + 1; c.brank[ce + 2] = 2 * br + 2; }
+    }
+    if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e - 2 * br;
 }
 
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
-template <bool LAK, bool STATE, bool PQ, int BS>
+// BND (quad P only): P has a boundary; tw / t of P are -1 where there is no
+// twin, and P's edges carry their boundary ranks.
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
+    static_assert(!BND || PQ, "the boundary path needs quad faces in P");
     // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores (consecutive
     // t) and the run-order reads (4 k's of a t, then the next t) are both free
     // of bank conflicts
@@ -217,6 +270,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         tw1_px = valid && (LAK || STATE) ? __ldg(p.tw + px) : 0;
     }
     const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
+    int br_x = 0, br_px = 0;                             // their boundary ranks
+    if (BND && valid) { br_x = __ldg(p.brank + eidp_x); br_px = __ldg(p.brank + eidp_px); }
 
     // face point of quad x
     float4 fp;
@@ -229,7 +284,9 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     // edge ids of C's corners 4x+k
     int e0, e1, e2, e3;
     if (!LAK) {
-        e0 = s1; e1 = d.N1 + nxx; e2 = d.N1 + x; e3 = t1x;
+        // a prev(x) edge without a twin: C's edge {e_in(x), v} is owned by
+        // corner 4x+3 itself, ranked after the 2 N1 interior owners
+        e0 = s1; e1 = d.N1 + nxx; e2 = d.N1 + x; e3 = (!BND || t1x >= 0) ? t1x : 2 * d.N1 + br_px;
     } else {
         int vnx, vpx, fx, ftw, ftwp;
         if (PQ) {
@@ -242,10 +299,12 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
             ftw = valid ? pf.face(tw1x) : 0;
             ftwp = valid ? pf.face(tw1_px) : 0;
         }
-        e0 = 4 * eidp_x + (Q.x > vnx);
-        e1 = 4 * eidp_x + 2 + (fx > ftw);
-        e2 = 4 * eidp_px + 2 + (fx > ftwp);
-        e3 = 4 * eidp_px + (Q.x > vpx);
+        // C's edges around P's edge e start at 4e - brank(e); a boundary edge
+        // has one face point, ranked 2
+        e0 = 4 * eidp_x - br_x + (Q.x > vnx);
+        e1 = 4 * eidp_x - br_x + 2 + ((!BND || tw1x >= 0) && fx > ftw);
+        e2 = 4 * eidp_px - br_px + 2 + ((!BND || tw1_px >= 0) && fx > ftwp);
+        e3 = 4 * eidp_px - br_px + (Q.x > vpx);
     }
     // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}: staged, then one coalesced run
     const int fpid = d.V + x;
@@ -269,7 +328,13 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         z.Z[2 * (int64_t)s1] = fp;
         z.Z[2 * (int64_t)s1 + 1] = LAK ? c3 : c1;
         if (LAK) z.T[s1] = Q.w;
-        else z.rot[t1x] = s1;
+        else if (!BND || t1x >= 0) z.rot[t1x] = s1;
+        if (BND && !LAK && tw1x < 0) z.rot[s1] = s1;      // no rotation across the boundary: a safe index
+        if (BND) {
+            z.bflag[s1] = (tw1x < 0) | ((tw1_px < 0) << 1);
+            z.bid[s1] = LAK ? Q.y : Q.w;
+            if (STATE && !LAK) z.bscan[s1] = tw1x < 0;
+        }
     }
 
     if constexpr (!PQ) {
@@ -327,8 +392,10 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         }
 
         if (STATE && valid) {
-            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, qnext(tw1x), qnext(tw1_px), s1, t1x, eidp_x, eidp_px);
+            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, BND && tw1x < 0 ? 0 : qnext(tw1x),
+                             BND && tw1_px < 0 ? 0 : qnext(tw1_px), s1, t1x, eidp_x, eidp_px, br_x, br_px);
             if (q == 0) c.sptr[d.V1 + (x >> 2)] = d.N1 + x;            // = N1 + 4 * face
+            if (BND && !LAK) c.brank[d.N1 + x] = d.B1;                 // C's face-point edges are interior
         }
 
         // P's edge through x, on the lane of its min->max half-edge: what k_g2
@@ -337,7 +404,9 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         // their face points are rebuilt from three gathered positions.
         const int u = __shfl_sync(0xffffffffu, Q.x, ln);
         const float4 Pu = shfl4(c0, ln), Fnh = shfl4(fp, ln);
-        if (valid && Q.x < u) {
+        if (BND && valid && tw1x < 0) {        // the only half-edge of a boundary edge owns it
+            boundary_edge<LAK, STATE>(d, c, R, Q.x, u, Q.y, br_x, c0, Pu, c1, c2, fp, Fnh);
+        } else if (valid && Q.x < u) {
             const int h2 = tw1x, nh2 = qnext(h2), fh2 = d.V1 + (h2 >> 2);
             const float4 Pf2 = ldg4(P, fh2);
             const int ei2 = __ldg(ids + 4 * (int64_t)h2 + 3), eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1);
@@ -350,8 +419,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
                 Fh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), Pu), c1), Pf2), Pi2), 4.0f);
                 Fnh2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), Po3), Pf2), c1), 4.0f);
             }
-            edge_point_vertex<LAK, STATE>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, fh2, c0, Pu, c1, c2, Pf2, fp, Fnh,
-                                          Fh2, Fnh2);
+            edge_point_vertex<LAK, STATE, BND>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, fh2, c0, Pu, c1, c2, Pf2, fp,
+                                               Fnh, Fh2, Fnh2, br_x);
         }
     }
 }
@@ -503,10 +572,51 @@ __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* 
 }
 
 // ---------------------------------------------------------------------------------------------
+// A vertex of P on C's boundary (a slot of its column has a half-edge without
+// a twin): 3/4 p + 1/8 of its boundary neighbours, the edge points of the two
+// P boundary edges at v.  SLAK: the first out-boundary slot's e_out, then the
+// first in-boundary slot's e_in (correctBoundaryS2, CatmullClarkKernels.cuh
+// :709-740); LAK: every boundary neighbour once in ascending edge id, which
+// for edge points of different P edges is ascending vertex id
+// (calculateExternalVertexUpdate, LAKCatmullClarkKernels.cuh:483-511).  yv
+// is returned unchanged for an interior vertex.
+template <bool LAK>
+__device__ __forceinline__ float4 boundary_vertex(const float* __restrict__ P, const SlotScratch& z, int b, int e,
+                                                  float4 Pv, float4 yv)
+{
+    int sb = -1, si = -1;
+    for (int s = b; s < e; ++s) {
+        const int f = __ldg(z.bflag + s);
+        if ((f & 1) && sb < 0) sb = s;
+        if ((f & 2) && si < 0) si = s;
+    }
+    if (sb < 0 && si < 0) return yv;
+    if (!LAK) {
+        if (sb >= 0) yv = f4_add(f4_mul(Pv, 0.75f), f4_mul(__ldg(z.Z + 2 * (int64_t)sb + 1), 0.125f));
+        if (si >= 0) yv = f4_add(yv, f4_mul(ldg4(P, __ldg(z.bid + si)), 0.125f));
+        return yv;
+    }
+    yv = f4_mul(Pv, 0.75f);
+    for (int last = -1;;) {            // out-neighbours' ids are in bid, in-neighbours' in T
+        int best = INT32_MAX;
+        for (int s = b; s < e; ++s) {
+            const int f = __ldg(z.bflag + s);
+            if (f & 1) { const int o = __ldg(z.bid + s); if (o > last && o < best) best = o; }
+            if (f & 2) { const int o = __ldg(z.T + s); if (o > last && o < best) best = o; }
+        }
+        if (best == INT32_MAX) break;
+        yv = f4_add(yv, f4_mul(ldg4(P, best), 0.125f));
+        last = best;
+    }
+    return yv;
+}
+
+// ---------------------------------------------------------------------------------------------
 // G3: one thread per vertex v of P.  Its column's records (written by k_g1 at
 // the column's slots) are contiguous, so the vertex point and, for SLAK, the
-// edge points of C's edges {v, e_out(x)} (ids = the slots) stream.
-template <bool LAK, bool STATE, int BS>
+// edge points of C's edges {v, e_out(x)} (ids = the slots) stream.  With a
+// boundary (BND), an edge {v, e_out(x)} without a twin gets the midpoint.
+template <bool LAK, bool STATE, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
                                            SlotScratch z, float* __restrict__ R, int compensated)
 {
@@ -525,12 +635,14 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         // arithmetic and its order are the loops' below)
         float4 zf[4], zn[4];
         int tt[4];                             // LAK: tail ids; SLAK: rot - b
+        int fl[4] = {0, 0, 0, 0};              // boundary flags
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k < n) {
                 zf[k] = __ldg(Z + 2 * (int64_t)(b + k));
                 zn[k] = __ldg(Z + 2 * (int64_t)(b + k) + 1);
                 tt[k] = LAK ? __ldg(z.T + b + k) : __ldg(z.rot + b + k) - b;
+                if (BND) fl[k] = __ldg(z.bflag + b + k);
             }
         }
         float4 acc = f4_zero();
@@ -546,6 +658,10 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
 #pragma unroll
             for (int k = 0; k < 4; ++k)
                 if (k < n) {
+                    if (BND && (fl[k] & 1)) {
+                        st4_cs(R, EPb + b + k, f4_mul(f4_add(Pv, zn[k]), 0.5f));
+                        continue;
+                    }
                     const int r = tt[k];
                     const float4 fr = r == 0 ? zf[0] : r == 1 ? zf[1] : r == 2 ? zf[2] : zf[3];
                     const float4 half = f4_mul(f4_add(zn[k], fr), 0.25f);
@@ -570,6 +686,7 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
                     if (k < n && rk[k] == r) acc = f4_add(acc, zn[k]);
             yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
         }
+        if (BND && (fl[0] | fl[1] | fl[2] | fl[3])) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
         st4(R, v, yv);
         if (STATE) c.sptr[v] = b;
         return;
@@ -594,6 +711,10 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         const int64_t EPb = (int64_t)d.V + d.N1;
         for_each_loaded(n, [&](int k) { return f4_add(zn(k), __ldg(Z + 2 * (int64_t)__ldg(z.rot + b + k))); },
                         [&](int k, float4 t) {
+                            if (BND && (__ldg(z.bflag + b + k) & 1)) {
+                                st4_cs(R, EPb + b + k, f4_mul(f4_add(Pv, zn(k)), 0.5f));
+                                return;
+                            }
                             const float4 ta = f4_mul(f4_add(Pv, zf(k)), 0.25f);
                             st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), ta), f4_mul(t, 0.25f)));
                         });
@@ -623,19 +744,32 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         if (comp) yv = vp_finish(sh, sl, Pv, n);
         else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
     }
+    if (BND) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
     st4(R, v, yv);
     if (STATE) c.sptr[v] = b;
 }
 
 // ---------------------------------------------------------------------------------------------
-// t of a general quad level feeding the fast path (SLAK): t[x] = slot[tw[prev x]]
+// t of a general level feeding the fast path (SLAK): t[x] = slot[tw[prev x]],
+// -1 where prev(x) has no twin
 template <bool QUAD>
 __global__ void k_export_t(Faces<QUAD> fc, int N, const int* __restrict__ slot, const int* __restrict__ tw,
                            int* __restrict__ t)
 {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= N) return;
-    t[x] = slot[tw[fc.prev(x)]];
+    const int tp = tw[fc.prev(x)];
+    t[x] = tp >= 0 ? slot[tp] : -1;
+}
+
+// 1 for each edge of a general level without a twin (H holds -1), the input of
+// the scan that gives the edges' boundary ranks to the first fast level
+__global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restrict__ isb)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int2 h = H[e];
+    isb[e] = (h.x < 0) | (h.y < 0);
 }
 
 }  // namespace slak

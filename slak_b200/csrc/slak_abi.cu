@@ -48,6 +48,7 @@ struct Level {
     float* o_verts = nullptr;
     int* o_ptr = nullptr;
     int* o_vals = nullptr;
+    int* scan_tmp = nullptr;       // fast level with a boundary (SLAK, state): scan of C's boundary edges
     // fast level: block size of k_g1, k_g2, k_g3 (chosen by the autotuner)
     int bs[3] = {256, 256, 256};
     int tuned = 0;                 // 0 default, 1 measured now, 2 from the tuning cache
@@ -72,6 +73,7 @@ struct Scratch {
         *tmp = nullptr;
     int2* H = nullptr;
     int *xslot = nullptr, *xtw = nullptr, *xt = nullptr;   // state export of a general quad level
+    int *xbrank = nullptr, *xisb = nullptr;                // ... with a boundary: edges' boundary ranks
 };
 
 size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -154,6 +156,9 @@ struct slak_plan {
     int64_t maxN = 0, maxV = 0, maxE = 0;
     bool any_poly = false;
     int64_t exN = 0, stN = 0, stV = 0, slN = 0, mid_ids = 0, mid_verts = 0;
+    int64_t exE = 0, stE = 0;        // edges of the exported / state levels (boundary ranks)
+    bool bnd_fast = false;           // some fast level has a parent with a boundary
+    int* bnd_tmp = nullptr;          // scan tiles for C's boundary ranks
     bool arena_owned = true;
     QState qs[2]{};
     SlotScratch slots{};
@@ -190,19 +195,23 @@ void carve_scratch(Carver& cv, Scratch& s, int64_t N, int64_t V, int64_t E, bool
     s.H = cv.take<int2>(E);
 }
 
-void carve_export(Carver& cv, Scratch& s, int64_t N)
+// E > 0: the exported level has a boundary, so its edges' boundary ranks go too
+void carve_export(Carver& cv, Scratch& s, int64_t N, int64_t E)
 {
     s.xslot = cv.take<int>(N);
     s.xtw = cv.take<int>(N);
     s.xt = cv.take<int>(N);
+    s.xbrank = E ? cv.take<int>(E + 1) : nullptr;
+    s.xisb = E ? cv.take<int>(E) : nullptr;
 }
 
-void carve_state(Carver& cv, QState& q, int64_t N, int64_t V)
+void carve_state(Carver& cv, QState& q, int64_t N, int64_t V, int64_t E)
 {
     q.sptr = cv.take<int>(V + 1);
     q.slot = cv.take<int>(N);
     q.tw = cv.take<int>(N);
     q.t = cv.take<int>(N);
+    q.brank = E ? cv.take<int>(E + 1) : nullptr;
 }
 
 // Topology of a level up to the edge-offset scan (needs no output buffers).
@@ -309,11 +318,12 @@ void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevSt
     lc.after("k_vp");
 }
 
-// One fast level: C = L (refined from its parent level Pl, whose state is L.in_state).
-template <bool LAK, bool STATE, bool PQ>
+// One fast level: C = L (refined from its parent level Pl, whose state is
+// L.in_state).  BND: Pl has a boundary (quad faces only).
+template <bool LAK, bool STATE, bool PQ, bool BND>
 void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc& lc)
 {
-    FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N};
+    FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N, (int)Pl.B};
     cudaStream_t str = lc.s;
     // compulsory bytes of each kernel: the level's corner ids and positions it
     // must read once, and the refined ids / positions it alone writes
@@ -321,9 +331,9 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g1<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state, L.out_state,
-                                                                    reinterpret_cast<int4*>(L.o_ids), L.o_verts,
-                                                                    L.slots);
+        k_g1<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
+                                                                         L.out_state, reinterpret_cast<int4*>(L.o_ids),
+                                                                         L.o_verts, L.slots);
     });
     lc.after("k_g1", 1, PQ ? g1b + g2b : g1b);
     if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
@@ -338,21 +348,26 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     }
     with_block(L.bs[2], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g3<LAK, STATE, BS><<<grid_for(Pl.V + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state, L.slots,
-                                                                     L.o_verts, comp ? 1 : 0);
+        k_g3<LAK, STATE, BS, BND><<<grid_for(Pl.V + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
+                                                                          L.slots, L.o_verts, comp ? 1 : 0);
     });
     lc.after("k_g3", 1, 16 * Pl.V + (LAK ? 0 : 16 * L.F));
+    if (BND && STATE && !LAK) {    // C's edges 0..N1-1 (P's slots): boundary ranks by a scan
+        int64_t nl = 0;
+        scan_exclusive(L.slots.bscan, L.out_state.brank, Pl.N, L.scan_tmp, str, &nl);
+        lc.after("scan(boundary)", (int)nl);
+    }
 }
 
-template <bool PQ>
+template <bool PQ, bool BND>
 void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool comp, Lc& lc)
 {
     if (lak) {
-        if (L.make_state) launch_fast_t<true, true, PQ>(Pl, L, pf, comp, lc);
-        else launch_fast_t<true, false, PQ>(Pl, L, pf, comp, lc);
+        if (L.make_state) launch_fast_t<true, true, PQ, BND>(Pl, L, pf, comp, lc);
+        else launch_fast_t<true, false, PQ, BND>(Pl, L, pf, comp, lc);
     } else {
-        if (L.make_state) launch_fast_t<false, true, PQ>(Pl, L, pf, comp, lc);
-        else launch_fast_t<false, false, PQ>(Pl, L, pf, comp, lc);
+        if (L.make_state) launch_fast_t<false, true, PQ, BND>(Pl, L, pf, comp, lc);
+        else launch_fast_t<false, false, PQ, BND>(Pl, L, pf, comp, lc);
     }
 }
 
@@ -360,8 +375,9 @@ void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool
 void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, bool comp, Lc& lc)
 {
     const bool lak = scheme == SLAK_SCHEME_LAK;
-    if (Pl.quad) launch_fast_p<true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
-    else launch_fast_p<false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
+    if (Pl.quad && Pl.B > 0) launch_fast_p<true, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else if (Pl.quad) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else launch_fast_p<false, false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     if (L.o_ptr) {   // LAK final level: quad offsets and corner positions
         k_quad_ptr_vals<<<grid_for(L.N), kBlock, 0, lc.s>>>((int)L.N, L.o_ptr, reinterpret_cast<int4*>(L.o_vals));
         lc.after("k_quad_ptr_vals");
@@ -405,6 +421,13 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
                 k_export_t<false><<<grid_for(L.N), kBlock, 0, str>>>(Faces<false>{L.ptr, p->s.cface}, (int)L.N,
                                                                      p->s.xslot, p->s.xtw, p->s.xt);
             lc.after("k_export_t");
+        }
+        if (L.export_state && L.B > 0) {     // the edges' boundary ranks
+            k_export_bflag<<<grid_for(L.E), kBlock, 0, str>>>((int)L.E, p->s.H, p->s.xisb);
+            lc.after("k_export_bflag");
+            int64_t n3 = 0;
+            scan_exclusive(p->s.xisb, p->s.xbrank, L.E, p->s.tmp, str, &n3);
+            lc.after("scan(boundary)", (int)n3);
         }
     }
     p->launches = nl;
@@ -526,7 +549,8 @@ int plan_levels(slak_plan* p)
             L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
             L.E = (L.N - L.B) / 2 + L.B;
             L.quad = true; L.poly_fn = false;
-            L.fast = !force_general && P.B == 0;     // closed parent, quad or polygon faces
+            // closed parents with quad or polygon faces; parents with a boundary need quad faces
+            L.fast = !force_general && (P.B == 0 || P.quad);
         }
         L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
         if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
@@ -540,11 +564,17 @@ int plan_levels(slak_plan* p)
     for (int i = 0; i < nlev; ++i) {
         Level& L = p->lv[i];
         if (L.fast && p->lv[i - 1].N > p->slN) p->slN = p->lv[i - 1].N;
-        if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) { L.export_state = true; if (L.N > p->exN) p->exN = L.N; }
+        if (L.fast && p->lv[i - 1].B > 0) p->bnd_fast = true;
+        if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) {
+            L.export_state = true;
+            if (L.N > p->exN) p->exN = L.N;
+            if (L.B > 0 && L.E > p->exE) p->exE = L.E;
+        }
         if (L.fast && i + 1 < nlev && p->lv[i + 1].fast) {
             L.make_state = true;
             if (L.N > p->stN) p->stN = L.N;
             if (L.V > p->stV) p->stV = L.V;
+            if (L.B > 0 && L.E > p->stE) p->stE = L.E;
         }
     }
     for (int i = 0; i + 1 < nlev; ++i) {
@@ -560,11 +590,20 @@ void plan_carve(slak_plan* p, Carver& cv)
 {
     const int nlev = (int)p->lv.size();
     carve_scratch(cv, p->s, p->maxN, p->maxV, p->maxE, p->any_poly);
-    if (p->exN) carve_export(cv, p->s, p->exN);
-    if (p->stN) { carve_state(cv, p->qs[0], p->stN, p->stV); carve_state(cv, p->qs[1], p->stN, p->stV); }
+    if (p->exN) carve_export(cv, p->s, p->exN, p->exE);
+    if (p->stN) {
+        carve_state(cv, p->qs[0], p->stN, p->stV, p->stE);
+        carve_state(cv, p->qs[1], p->stN, p->stV, p->stE);
+    }
     if (p->slN) {
         p->slots.Z = cv.take<float4>(2 * p->slN);
         p->slots.T = p->slots.rot = cv.take<int>(p->slN);
+        if (p->bnd_fast) {
+            p->slots.bflag = cv.take<int>(p->slN);
+            p->slots.bid = cv.take<int>(p->slN);
+            p->slots.bscan = cv.take<int>(p->slN);
+            p->bnd_tmp = cv.take<int>(scan_tiles(p->slN) + 2);
+        }
     }
     for (int k = 0; k < 2; ++k) {
         p->ping_ids[k] = nlev > 1 ? cv.take<int>(p->mid_ids) : nullptr;
@@ -608,10 +647,11 @@ void plan_wire(slak_plan* p)
         Level& L = p->lv[i];
         if (!L.fast) continue;
         const Level& P = p->lv[i - 1];
-        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.xslot, p->s.xtw, p->s.xt};
+        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.xslot, p->s.xtw, p->s.xt, p->s.xbrank};
         else L.in_state = P.out_state;
         if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
         L.slots = p->slots;
+        L.scan_tmp = p->bnd_tmp;
     }
 }
 
@@ -695,8 +735,9 @@ std::string tune_key(const slak_plan* p, int li)
     const int sclass = share4 < 0.5 ? 0 : share4 < 0.9 ? 50 : 90;
     const int fb = (int)std::floor(std::log2((double)std::max<int64_t>(L.F, 1)));
     char buf[96];
-    std::snprintf(buf, sizeof buf, "%s/%s/%s/q2^%d/vmax%d/v4_%d", p->scheme == SLAK_SCHEME_LAK ? "lak" : "slak",
-                  P.quad ? "quad" : "poly", L.make_state ? "state" : "last", fb, vclass, sclass);
+    std::snprintf(buf, sizeof buf, "%s/%s%s/%s/q2^%d/vmax%d/v4_%d", p->scheme == SLAK_SCHEME_LAK ? "lak" : "slak",
+                  P.quad ? "quad" : "poly", P.B > 0 ? "-open" : "", L.make_state ? "state" : "last", fb, vclass,
+                  sclass);
     return buf;
 }
 

@@ -83,3 +83,29 @@ def closed(mesh) -> bool:
     nxt = np.where(c + 1 < end, c + 1, start)
     a, b = mesh.ids.astype(np.int64), mesh.ids[nxt].astype(np.int64)
     return bool(np.isin(a * mesh.nverts + b, b * mesh.nverts + a).all())
+
+
+def cut_mesh(mesh, keep_face) -> Mesh:
+    """The faces of `mesh` where keep_face[f] is true, unused vertices dropped:
+    an open mesh (boundaries where faces were removed)."""
+    ptr = mesh.ptr if mesh.ptr is not None else np.arange(mesh.nfaces + 1, dtype=np.int64) * 4
+    keep = np.flatnonzero(keep_face)
+    orders = np.diff(ptr)[keep]
+    corners = np.concatenate([np.arange(ptr[f], ptr[f + 1]) for f in keep])
+    ids = mesh.ids[corners].astype(np.int64)
+    used = np.unique(ids)
+    remap = np.full(mesh.nverts, -1, np.int64)
+    remap[used] = np.arange(used.size)
+    nptr = np.concatenate([[0], np.cumsum(orders)])
+    return from_arrays(nptr, remap[ids], np.asarray(mesh.verts, np.float32)[used, :3])
+
+
+def open_mixed(W=64, H=48, seed=5) -> Mesh:
+    """The mixed-polygon torus with a sector around the major axis removed:
+    polygons of 3-8 sides and two boundary loops."""
+    m = meshgen.mixed_torus(W, H, 0.05, 0.03, 0.005, seed=seed)
+    ptr = m.ptr
+    cx = np.add.reduceat(np.asarray(m.verts, np.float64)[m.ids, 0], ptr[:-1]) / np.diff(ptr)
+    cy = np.add.reduceat(np.asarray(m.verts, np.float64)[m.ids, 1], ptr[:-1]) / np.diff(ptr)
+    ang = np.arctan2(cy, cx)
+    return cut_mesh(m, ~((ang > 0.0) & (ang < 1.2)))

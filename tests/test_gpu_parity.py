@@ -12,7 +12,7 @@ import oracle
 from slak_b200 import api, meshgen
 from slak_b200.mesh import LAK, QUAD, SLAK
 
-from meshes import small_set, open_grid
+from meshes import open_grid, open_mixed, small_set
 
 pytestmark = pytest.mark.gpu
 
@@ -152,4 +152,29 @@ def test_fast_path_compensated_matches_general_compensated():
     m = meshgen.workload("cylinder").mesh
     a = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED)
     b = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+    assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
+
+
+OPEN = [("grid", lambda: open_grid(48, 40), 4), ("mixed_cut", lambda: open_mixed(), 4),
+        ("grid_thin", lambda: open_grid(200, 1), 3)]
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name,make,levels", OPEN, ids=[c[0] for c in OPEN])
+def test_open_meshes_bit_exact(name, make, levels, scheme):
+    """Meshes with a boundary: closed-form levels with boundary ranks and the
+    boundary rules, bit for bit against the oracle and the general path."""
+    mesh = make()
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    got, ref = _check(mesh, levels, scheme)
+    assert _bits_equal(got.verts, ref.verts)
+    gen = api.subdivide(mesh, levels, scheme, api._abi.PLAN_GENERAL)
+    assert np.array_equal(got.ids, gen.ids) and _bits_equal(got.verts, gen.verts)
+
+
+def test_open_mesh_compensated_matches_general():
+    m = open_mixed()
+    a = api.subdivide(m, 4, SLAK, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(m, 4, SLAK, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
     assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
