@@ -91,6 +91,20 @@ def capped_cylinder(segs: int = 64, rings: int = 32, jitter: float = 0.001, seed
     return _call(_load().mg_capped_cylinder, segs, rings, jitter, seed)
 
 
+def open_grid(W: int, H: int, jitter: float = 0.005, seed: int = 16) -> Mesh:
+    """A flat W x H quad patch with height noise: an open mesh, its boundary a
+    single loop of 2(W+H) edges (the boundary rules of both schemes)."""
+    from .mesh import from_arrays
+    rng = np.random.default_rng(seed)
+    i, j = np.meshgrid(np.arange(W + 1), np.arange(H + 1), indexing="ij")
+    xyz = np.stack([i.ravel() / W, j.ravel() / H, jitter * rng.standard_normal(i.size)], 1)
+    vid = lambda a, b: a * (H + 1) + b
+    a, b = np.meshgrid(np.arange(W), np.arange(H), indexing="ij")
+    a, b = a.ravel(), b.ravel()
+    faces = np.stack([vid(a, b), vid(a + 1, b), vid(a + 1, b + 1), vid(a, b + 1)], 1)
+    return from_arrays(np.arange(W * H + 1) * 4, faces.reshape(-1), xyz.astype(np.float32))
+
+
 @dataclasses.dataclass
 class Workload:
     name: str
@@ -108,6 +122,8 @@ def workload(name: str) -> Workload:
         return Workload(name, mixed_torus(512, 512, 0.05, 0.03, 0.005, seed=13), 4, (1, 0))
     if name == "cylinder":
         return Workload(name, capped_cylinder(64, 32, 0.001, seed=15), 7, (1, 0))
+    if name == "grid512":           # an open mesh (boundary rules), beside the closed configurations
+        return Workload(name, open_grid(512, 512), 4, (1, 0))
     raise KeyError(name)
 
 
