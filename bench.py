@@ -332,9 +332,21 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
 
 def batch_shard(count, rank=0, ws=1):
     """Specs of this rank's meshes of the 2,000-mesh batch (seeded kinds, sizes
-    and level counts): with ws > 1 each rank takes every ws-th mesh."""
+    and level counts), in batch order.  With ws > 1 the meshes are split by
+    predicted output (faces x 4^(levels-1), the refined quads up to a constant):
+    largest first, each to the rank with the least so far (ties to the lowest
+    rank), so every rank refines about the same number of quads."""
     from slak_b200 import meshgen
-    return [it for k, it in enumerate(meshgen.batch_specs(count)) if k % ws == rank]
+    specs = meshgen.batch_specs(count)
+    if ws == 1:
+        return specs
+    load = [0] * ws
+    owner = [0] * len(specs)
+    for k in sorted(range(len(specs)), key=lambda k: (-specs[k].faces * 4 ** (specs[k].levels - 1), k)):
+        r = min(range(ws), key=lambda r: (load[r], r))
+        owner[k] = r
+        load[r] += specs[k].faces * 4 ** (specs[k].levels - 1)
+    return [it for k, it in enumerate(specs) if owner[k] == rank]
 
 
 def batch_workload(count, rank=0, ws=1):

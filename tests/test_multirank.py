@@ -1,7 +1,7 @@
 """The multi-GPU form is replicas only: every rank refines its own meshes and
 the only collectives are the timing reductions.  These run as two gloo ranks
 on the CPU: max-over-ranks timing, and the partition of the batched workload
-(every mesh on exactly one rank, sizes summing to the whole)."""
+(every mesh on exactly one rank, the predicted work balanced)."""
 import os
 import socket
 import sys
@@ -51,8 +51,9 @@ def test_two_gloo_ranks_time_and_partition():
     whole = [(it.kind, it.faces, it.levels, it.seed) for it in bench.batch_shard(2000)]
     shards = [s for _, _, s in res]
     assert len(shards[0]) + len(shards[1]) == len(whole)
-    merged = [None] * len(whole)
-    for r, sh in enumerate(shards):
-        for k, item in enumerate(sh):
-            merged[2 * k + r] = item
-    assert merged == whole
+    assert sorted(shards[0] + shards[1]) == sorted(whole)          # a partition of the batch
+    for sh in shards:                                               # each shard keeps batch order
+        assert sh == [it for it in whole if it in sh]
+    work = [sum(f * 4 ** (lv - 1) for _, f, lv, _ in sh) for sh in shards]
+    biggest = max(f * 4 ** (lv - 1) for _, f, lv, _ in whole)
+    assert abs(work[0] - work[1]) <= biggest                        # balanced to within one mesh
