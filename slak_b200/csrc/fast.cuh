@@ -222,14 +222,13 @@ __device__ __forceinline__ void boundary_edge(const FastDims& d, QState& c, floa
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
-// BND (quad P only): P has a boundary; tw / t of P are -1 where there is no
-// twin, and P's edges carry their boundary ranks.
+// BND: P has a boundary; tw / t of P are -1 where there is no twin, and P's
+// edges carry their boundary ranks.
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
 {
-    static_assert(!BND || PQ, "the boundary path needs quad faces in P");
     // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores (consecutive
     // t) and the run-order reads (4 k's of a t, then the next t) are both free
     // of bank conflicts
@@ -253,7 +252,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     if constexpr (PQ) c3 = shfl4(c1, (threadIdx.x & 31 & ~3) | ((x + 3) & 3));
     else c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
-    if (valid && (LAK || STATE || PQ)) tw1x = __ldg(p.tw + x);
+    if (valid && (LAK || STATE || PQ || BND)) tw1x = __ldg(p.tw + x);
     if (valid) s1 = __ldg(p.slot + x);
     if (valid && !LAK) t1x = __ldg(p.t + x);
     const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         const int fb = valid ? __ldg(pf.ptr + f) : 0, fe = valid ? __ldg(pf.ptr + f + 1) : 1;
         nxx = x + 1 == fe ? fb : x + 1;
         px = x == fb ? fe - 1 : x - 1;
-        tw1_px = valid && (LAK || STATE) ? __ldg(p.tw + px) : 0;
+        tw1_px = valid && (LAK || STATE || BND) ? __ldg(p.tw + px) : 0;
     }
     const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
     int br_x = 0, br_px = 0;                             // their boundary ranks
@@ -296,8 +295,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
             vnx = valid ? __ldg(ids + 4 * (int64_t)nxx) : 0;
             vpx = valid ? __ldg(ids + 4 * (int64_t)px) : 0;
             fx = Q.z - d.V1;
-            ftw = valid ? pf.face(tw1x) : 0;
-            ftwp = valid ? pf.face(tw1_px) : 0;
+            ftw = valid && tw1x >= 0 ? pf.face(tw1x) : 0;        // no face across a boundary
+            ftwp = valid && tw1_px >= 0 ? pf.face(tw1_px) : 0;
         }
         // C's edges around P's edge e start at 4e - brank(e); a boundary edge
         // has one face point, ranked 2
@@ -340,8 +339,9 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     if constexpr (!PQ) {
         // polygon P: P's face points and C's inner edge points are k_gf's
         if (STATE && valid) {
-            const int ntw = pf.next(tw1x), ntwp = pf.next(tw1_px);
-            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, ntw, ntwp, s1, t1x, eidp_x, eidp_px);
+            const int ntw = BND && tw1x < 0 ? 0 : pf.next(tw1x), ntwp = BND && tw1_px < 0 ? 0 : pf.next(tw1_px);
+            write_state<LAK>(d, c, x, nxx, px, tw1x, tw1_px, ntw, ntwp, s1, t1x, eidp_x, eidp_px, br_x, br_px);
+            if (BND && !LAK) c.brank[d.N1 + x] = d.B1;                 // C's face-point edges are interior
         }
     } else {
         // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
@@ -426,6 +426,36 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
 }
 
 // ---------------------------------------------------------------------------------------------
+// The vertex point of P's face point with the face's k > 4 corners b..e-1 under
+// SLAK_PLAN_COMPENSATED: the same terms in the same order as the general path's
+// compensated vertex points (k_vp_slak / k_vp_lak): TwoSum sums, exact-remainder
+// quotients, one rounding.  SLAK: e_in(x) then FP(x); LAK: FP(x), then the
+// tails e_out(x) in ascending id.
+template <bool LAK>
+__device__ __noinline__ float4 face_vertex_compensated(const int* __restrict__ ids, const float* __restrict__ P,
+                                                       const float* __restrict__ FP, int b, int e, float4 c2)
+{
+    float4 sh = f4_zero(), sl = f4_zero();
+    if (!LAK) {
+        for (int x = b; x < e; ++x) dd_acc(sh, sl, ldg4(P, __ldg(ids + 4 * (int64_t)x + 3)));
+        for (int x = b; x < e; ++x) dd_acc(sh, sl, ldg4(FP, x));
+    } else {
+        for (int x = b; x < e; ++x) dd_acc(sh, sl, ldg4(FP, x));
+        for (int last = -1;;) {
+            int xm = INT32_MAX;
+            for (int x = b; x < e; ++x) {
+                const int ti = __ldg(ids + 4 * (int64_t)x + 1);
+                if (ti > last && ti < xm) xm = ti;
+            }
+            if (xm == INT32_MAX) break;
+            dd_acc(sh, sl, ldg4(P, xm));
+            last = xm;
+        }
+    }
+    return vp_finish(sh, sl, c2, e - b);
+}
+
+// ---------------------------------------------------------------------------------------------
 // GF (polygon P only): one thread per face g of P, with k corners x = ptr[g] ..
 // ptr[g+1]-1.  The vertex point of P's face point V1 + g (its column in C is
 // corners 4x+2, ascending) and, for SLAK, the edge points N1 + x of C's inner
@@ -433,7 +463,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
 // are quads.  Same formulas and order, with n = k.
 template <bool LAK, bool STATE>
 __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
-                                               const float* __restrict__ P, QState c, float* __restrict__ R)
+                                               const float* __restrict__ P, QState c, float* __restrict__ R,
+                                               int compensated)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.F1) return;
@@ -492,6 +523,7 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
                 }
             yv = f4_div_z(f4_add(f4_div_z(acc, (float)k), f4_mul(c2, __fadd_rn((float)k, -2.0f))), (float)k);
         }
+        if (compensated && k > 4) yv = face_vertex_compensated<LAK>(ids, P, FP, b, e, c2);
         st4(R, (int64_t)d.V1 + g, yv);
         if (STATE) c.sptr[d.V1 + g] = d.N1 + b;
         return;
@@ -523,6 +555,7 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
         }
         yv = f4_div_z(f4_add(f4_div_z(acc, (float)k), f4_mul(c2, __fadd_rn((float)k, -2.0f))), (float)k);
     }
+    if (compensated && k > 4) yv = face_vertex_compensated<LAK>(ids, P, FP, b, e, c2);
     st4(R, (int64_t)d.V1 + g, yv);
     if (STATE) c.sptr[d.V1 + g] = d.N1 + b;
 }
@@ -536,7 +569,7 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
 // of quads h and next(h)) are coalesced loads or shuffles, and only the twin
 // face's three (its face point, C's face points of quads h2 and next(h2)) are
 // gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
-template <bool LAK, bool STATE, bool PQ, int BS>
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
 {
@@ -561,14 +594,22 @@ __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* 
         nh = x + 1 == fe ? fb : x + 1;
         u = __ldg(ids + 4 * (int64_t)nh);
     }
-    if (!valid || Q.x >= u) return;              // not the min->max half-edge of its edge
+    // the edge's owner: its min->max half-edge, or its only one (BND: no twin)
+    if (!valid || (Q.x >= u && !(BND && h2 < 0))) return;
     if (!PQ) Fnh = ldg4(FP, nh);
+    const int br = BND ? __ldg(p.brank + (Q.y - d.V1 - d.F1)) : 0;
+    if (BND && h2 < 0) {
+        boundary_edge<LAK, STATE>(d, c, R, Q.x, u, Q.y, br, ldg4(P, Q.x), ldg4(P, u), ldg4(P, Q.y), ldg4(P, Q.z), Fh,
+                                  Fnh);
+        return;
+    }
     const int h = x, nh2 = pf.next(h2);
     const int ve = Q.y, fh = Q.z, fh2 = d.V1 + pf.face(h2);
     const float4 Pv = ldg4(P, Q.x), Pu = ldg4(P, u);
     const float4 Pe = ldg4(P, ve), Pf = ldg4(P, fh), Pf2 = ldg4(P, fh2);
     const float4 Fh2 = ldg4(FP, h2), Fnh2 = ldg4(FP, nh2);
-    edge_point_vertex<LAK, STATE>(d, c, R, h, nh, h2, nh2, ve, fh, fh2, Pv, Pu, Pe, Pf, Pf2, Fh, Fnh, Fh2, Fnh2);
+    edge_point_vertex<LAK, STATE, BND>(d, c, R, h, nh, h2, nh2, ve, fh, fh2, Pv, Pu, Pe, Pf, Pf2, Fh, Fnh, Fh2, Fnh2,
+                                       br);
 }
 
 // ---------------------------------------------------------------------------------------------

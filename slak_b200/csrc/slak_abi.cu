@@ -337,12 +337,13 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     });
     lc.after("k_g1", 1, PQ ? g1b + g2b : g1b);
     if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
-        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts);
+        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts,
+                                                              comp ? 1 : 0);
         lc.after("k_gf");
         with_block(L.bs[1], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            k_g2<LAK, STATE, PQ, BS><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
-                                                                        L.out_state, L.o_verts);
+            k_g2<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
+                                                                             L.out_state, L.o_verts);
         });
         lc.after("k_g2", 1, g2b);
     }
@@ -377,6 +378,7 @@ void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, 
     const bool lak = scheme == SLAK_SCHEME_LAK;
     if (Pl.quad && Pl.B > 0) launch_fast_p<true, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.quad) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else if (Pl.B > 0) launch_fast_p<false, true>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     else launch_fast_p<false, false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     if (L.o_ptr) {   // LAK final level: quad offsets and corner positions
         k_quad_ptr_vals<<<grid_for(L.N), kBlock, 0, lc.s>>>((int)L.N, L.o_ptr, reinterpret_cast<int4*>(L.o_vals));
@@ -549,8 +551,7 @@ int plan_levels(slak_plan* p)
             L.F = P.Fo; L.V = P.Vo; L.N = P.No; L.B = 2 * P.B;
             L.E = (L.N - L.B) / 2 + L.B;
             L.quad = true; L.poly_fn = false;
-            // closed parents with quad or polygon faces; parents with a boundary need quad faces
-            L.fast = !force_general && (P.B == 0 || P.quad);
+            L.fast = !force_general;     // any parent: closed or open, quad or polygon faces
         }
         L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
         if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;

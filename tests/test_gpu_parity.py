@@ -148,10 +148,16 @@ def test_fast_path_equals_general_path(name, levels, scheme):
         assert np.array_equal(fast.ptr, gen.ptr) and np.array_equal(fast.vals, gen.vals)
 
 
-def test_fast_path_compensated_matches_general_compensated():
-    m = meshgen.workload("cylinder").mesh
-    a = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED)
-    b = api.subdivide(m, 5, SLAK, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name", ["cylinder", "mixed"])
+def test_fast_path_compensated_matches_general_compensated(name, scheme):
+    """Compensated vertex points on both paths, including the polygon faces of
+    more than 4 corners (their face points' vertex points, k_gf)."""
+    m = (meshgen.workload("cylinder").mesh if name == "cylinder"
+         else meshgen.mixed_torus(64, 48, 0.05, 0.03, 0.005, seed=8))
+    lv = 5 if name == "cylinder" else 4
+    a = api.subdivide(m, lv, scheme, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(m, lv, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
     assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
 
 
@@ -173,8 +179,9 @@ def test_open_meshes_bit_exact(name, make, levels, scheme):
     assert np.array_equal(got.ids, gen.ids) and _bits_equal(got.verts, gen.verts)
 
 
-def test_open_mesh_compensated_matches_general():
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+def test_open_mesh_compensated_matches_general(scheme):
     m = open_mixed()
-    a = api.subdivide(m, 4, SLAK, api._abi.PLAN_COMPENSATED)
-    b = api.subdivide(m, 4, SLAK, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+    a = api.subdivide(m, 4, scheme, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(m, 4, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
     assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
