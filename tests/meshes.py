@@ -109,3 +109,18 @@ def open_mixed(W=64, H=48, seed=5) -> Mesh:
     cy = np.add.reduceat(np.asarray(m.verts, np.float64)[m.ids, 1], ptr[:-1]) / np.diff(ptr)
     ang = np.arctan2(cy, cx)
     return cut_mesh(m, ~((ang > 0.0) & (ang < 1.2)))
+
+
+def bowtie(n=4) -> Mesh:
+    """Two open n x n grids sharing one corner vertex: a boundary vertex with
+    two boundary loops through it (two out- and two in-boundary half-edges)."""
+    a = open_grid(n, n)
+    va = np.asarray(a.verts, np.float32)[:, :3]
+    shared = n * (n + 1) + n                   # corner (n, n) of grid a
+    vb = va + np.array([n, n, 0.5], np.float32)
+    # grid b's corner (0, 0) (vertex 0) is grid a's corner (n, n)
+    remap = np.arange(va.shape[0]) + va.shape[0] - 1
+    remap[0] = shared
+    ids = np.concatenate([a.ids, remap[a.ids]])
+    verts = np.concatenate([va, vb[1:]])
+    return from_arrays(np.arange(2 * a.nfaces + 1) * 4, ids, verts)

@@ -10,7 +10,7 @@ import pytest
 import oracle
 from slak_b200.mesh import LAK, QUAD, SLAK, Mesh
 
-from meshes import fan_disk, open_grid
+from meshes import bowtie, fan_disk, open_grid
 
 
 def qn(x):
@@ -135,7 +135,8 @@ def _quad_level(mesh, scheme):
                 r.nfaces, 4, True)
 
 
-CASES = [("grid", lambda: open_grid(5, 4)), ("fan", lambda: fan_disk(7)), ("grid_wide", lambda: open_grid(9, 2))]
+CASES = [("grid", lambda: open_grid(5, 4)), ("fan", lambda: fan_disk(7)), ("grid_wide", lambda: open_grid(9, 2)),
+         ("bowtie", lambda: bowtie())]
 
 
 @pytest.mark.parametrize("scheme", [SLAK, LAK])

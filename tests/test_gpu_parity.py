@@ -12,7 +12,7 @@ import oracle
 from slak_b200 import api, meshgen
 from slak_b200.mesh import LAK, QUAD, SLAK
 
-from meshes import open_grid, open_mixed, small_set
+from meshes import bowtie, open_grid, open_mixed, small_set
 
 pytestmark = pytest.mark.gpu
 
@@ -185,3 +185,46 @@ def test_open_mesh_compensated_matches_general(scheme):
     a = api.subdivide(m, 4, scheme, api._abi.PLAN_COMPENSATED)
     b = api.subdivide(m, 4, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
     assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
+
+
+def test_bowtie_lak_bit_exact():
+    """Two boundary loops through one vertex.  LAK's boundary vertex rule
+    adds 1/8 of every boundary neighbour (prepare/calculateExternalVertexUpdate,
+    LAKCatmullClarkKernels.cuh:464-511), well defined at such a vertex."""
+    mesh = bowtie().with_quad_ptr()
+    got, ref = _check(mesh, 3, LAK)
+    assert _bits_equal(got.verts, ref.verts)
+    gen = api.subdivide(mesh, 3, LAK, api._abi.PLAN_GENERAL)
+    assert np.array_equal(got.ids, gen.ids) and _bits_equal(got.verts, gen.verts)
+
+
+def test_bowtie_slak_differs_only_where_the_reference_races():
+    """SLAK at a vertex X with two boundary loops: correctBoundaryS1/S2
+    (CatmullClarkKernels.cuh:689-740) send every boundary half-edge of X to
+    X's first one, so the second boundary edge keeps its interior edge point
+    and both of X's S2 updates land on the first neighbour, and S2's plain
+    read-modify-write races where two threads update one vertex.  The CUDA
+    path applies the boundary rule per half-edge (first out- and first
+    in-boundary slot of each vertex): topology is bit-exact, positions differ
+    only at X, the heads of X's boundary half-edges and their edge points."""
+    mesh = bowtie()
+    got, ref = _check(mesh, 1, SLAK)
+    ids = np.asarray(mesh.ids, np.int64)
+    c = np.arange(ids.size)
+    nxt = (c & ~3) | ((c + 1) & 3)
+    pairs = set(zip(ids.tolist(), ids[nxt].tolist()))
+    bnd = np.array([(int(b), int(a)) not in pairs for a, b in zip(ids, ids[nxt])])
+    x = np.bincount(ids[bnd]).argmax()
+    assert np.bincount(ids[bnd])[x] == 2
+    cx = c[bnd & (ids == x)]
+    allowed = {int(x)} | set(ids[nxt[cx]].tolist()) | set(np.asarray(got.ids)[4 * cx + 1].tolist())
+    a = np.asarray(got.verts, np.float32).view(np.uint32)
+    b = np.asarray(ref.verts, np.float32).view(np.uint32)
+    diff = set(np.nonzero((a != b).any(1))[0].tolist())
+    assert x in diff and diff <= allowed, (diff, allowed)
+    for lv in (2, 3):                     # the closed-form levels apply the same rule as the general path
+        fast = api.subdivide(mesh, lv, SLAK)
+        gen = api.subdivide(mesh, lv, SLAK, api._abi.PLAN_GENERAL)
+        ref = oracle.subdivide(mesh, lv, SLAK)
+        assert np.array_equal(fast.ids, ref.ids) and np.array_equal(fast.ids, gen.ids)
+        assert _bits_equal(fast.verts, gen.verts)
