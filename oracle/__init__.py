@@ -38,13 +38,20 @@ def lib():
         L.or_level.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_subdivide.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.or_mesh_free.argtypes = [P]
+        L.or_set_threads.argtypes = [ctypes.c_int]
         L.or_level.restype = L.or_subdivide.restype = L.or_num_threads.restype = ctypes.c_int
+        L.or_set_threads.restype = ctypes.c_int
         _lib = L
     return _lib
 
 
 def num_threads() -> int:
     return lib().or_num_threads()
+
+
+def set_threads(n: int) -> int:
+    """Thread count of later calls (n <= 0: the OpenMP default); returns it."""
+    return lib().or_set_threads(int(n))
 
 
 class Result:

@@ -44,6 +44,21 @@ int or_num_threads(void)
 #endif
 }
 
+/* Thread count of the following calls (n <= 0: the OpenMP default); returns
+ * the count now in effect.  Used to time the single-thread baseline. */
+int or_set_threads(int n)
+{
+#ifdef _OPENMP
+    static int dflt = 0;
+    if (!dflt) dflt = omp_get_max_threads();
+    omp_set_num_threads(n > 0 ? n : dflt);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
 /* ------------------------------------------------------------------------- */
 /* small helpers                                                              */
 

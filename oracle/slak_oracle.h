@@ -50,6 +50,10 @@ void or_mesh_free(or_mesh* m);
 /* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
 int  or_num_threads(void);
 
+/* Set the thread count of later calls (n <= 0: back to the OpenMP default);
+ * returns the count in effect. */
+int  or_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif

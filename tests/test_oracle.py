@@ -105,6 +105,23 @@ def test_deterministic():
     assert np.array_equal(a.ids, b.ids) and np.array_equal(a.verts.view(np.uint32), b.verts.view(np.uint32))
 
 
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+def test_single_thread_same_bits(scheme):
+    """The single-thread timing of the CPU baseline runs the same arithmetic:
+    one thread and the OpenMP default give identical results."""
+    name, mesh, levels = small_set()[8]
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    a = oracle.subdivide(mesh, levels, scheme)
+    assert oracle.set_threads(1) == 1
+    try:
+        b = oracle.subdivide(mesh, levels, scheme)
+    finally:
+        oracle.set_threads(0)
+    assert oracle.num_threads() >= 1
+    assert np.array_equal(a.ids, b.ids) and np.array_equal(a.verts.view(np.uint32), b.verts.view(np.uint32))
+
+
 def _slak_numbering_pure_python(mesh):
     """Independent pure-Python statement of the SLAK edge numbering rule
     (adjacency slots in corner order, owner = min->max half-edge or the only
