@@ -39,6 +39,8 @@ HBM_FALLBACK_GBS = 6650.0
 # (profiles/k_g_fast_levels_mixed384_slak.txt: k_g1 of the last level, SLAK,
 # per quad of the level it refines); scaled by the units of the bench's launch.
 TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 183.03}
+# B200 HBM3e datasheet bandwidth (DGX figure), reported beside the measured peak
+HBM_NOMINAL_GBS = 8000.0
 
 
 def _peaks():
@@ -251,6 +253,7 @@ def run_ours(args, dist, rank, ws):
         "tuning": tuning,
         "pipeline_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                               "frac": achieved / peak, "peak_kind": peak_kind,
+                              "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
                               "algorithmic_bytes": alg_bytes},
         "e2e": e2e,
         "clocks": clk.summary(),
@@ -294,7 +297,8 @@ def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush):
     dom = max(table, key=lambda t: t["ms"])
     achieved = dom["GB/s"] or 0.0
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "kernel": dom["kernel"], "level": dom["level"],
+            "frac": achieved / peak, "frac_of_nominal": achieved / HBM_NOMINAL_GBS, "traffic": None,
+            "kernel": dom["kernel"], "level": dom["level"],
             "kernel_ms": dom["ms"], "kernel_share": dom["share"], "peak_kind": f"{peak_kind} (copy bandwidth)",
             "algorithmic_bytes_per_launch": dom["algorithmic_bytes"]}
     return roof, sorted(table, key=lambda t: -t["ms"])
