@@ -224,6 +224,43 @@ int slak_plan_tuning(const slak_plan* plan, int level, slak_tuning* out);
 int slak_autotune_reset(void);    /* forget the in-process cache (the file is kept) */
 
 /*
+ * Semi-sharp creases.  The reference declares this step but does not implement
+ * it: "if (has_creases && !creases_decayed) time += handleCreases(...)" is
+ * commented out in LibSource/device/CatmullClarkImpl.cu:94-96 and :296-298 and
+ * LibSource/device/LAKCatmullClarkImpl.cu:240-242.  The rules are those of
+ * DeRose, Kass and Truong (SIGGRAPH 1998), with sharpness decaying by one per
+ * level.  Both schemes use the same rules.
+ *  - Edge points. An edge of sharpness s >= 1 becomes the midpoint of its
+ *    ends. For 0 < s < 1 the result is smooth * (1 - s) + midpoint * s.
+ *  - Vertex points. Let k be the number of crease edges at a vertex and
+ *    w = min(1, their mean sharpness). With k == 2 the vertex takes the crease
+ *    rule (3/4 p + 1/8 p_o1) + 1/8 p_o2, other ends in ascending id. With
+ *    k >= 3, or on a boundary, it is a corner (p unchanged). With k == 1 it
+ *    stays smooth. The sharp result is blended with the smooth one by w.
+ *  - Child edges. The two child edges of a crease edge carry s - 1.
+ *
+ * crease_verts holds 2 * ncreases vertex ids (the pairs {a, b}).
+ * crease_sharpness holds ncreases floats. Both arrays are in device memory and
+ * are copied into the plan at creation.
+ *  - A pair on a boundary edge is ignored, since the boundary is already
+ *    sharp. So is a pair with sharpness <= 0.
+ *  - A pair that is not an edge of the input, or an edge named twice, makes
+ *    the execution's status SLAK_ERR_BAD_MESH.
+ *  - A sharpness that is not finite gives SLAK_ERR_INVALID_ARG.
+ *
+ * The crease pass runs after each level that has a live crease. It needs four
+ * launches, and a mesh without creases pays nothing.
+ * slak_subdivide_creased is slak_subdivide with creases. It uses no workspace
+ * cache.
+ */
+int slak_plan_create_creased(const slak_mesh* cmesh, int target_level, int scheme, int flags,
+                             const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                             slak_stream_t stream, slak_plan** plan);
+int slak_subdivide_creased(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
+                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                           slak_stream_t stream);
+
+/*
  * Batches: many meshes, each with its own target level, refined by one call
  * (what the reference's config-file loop does one mesh at a time,
  * source/main.cpp:84-113).  Each mesh's result is exactly slak_subdivide's on

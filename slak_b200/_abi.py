@@ -11,6 +11,8 @@ import os
 from . import _paths
 
 SLAK_OK = 0
+SLAK_ERR_INVALID_ARG, SLAK_ERR_CUDA, SLAK_ERR_OOM, SLAK_ERR_BAD_MESH = 1, 2, 3, 4
+SLAK_ERR_TIMEOUT, SLAK_ERR_UNSUPPORTED, SLAK_ERR_NOT_READY = 5, 6, 7
 STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: "SLAK_ERR_OOM",
                 4: "SLAK_ERR_BAD_MESH", 5: "SLAK_ERR_TIMEOUT", 6: "SLAK_ERR_UNSUPPORTED", 7: "SLAK_ERR_NOT_READY"}
 
@@ -19,7 +21,7 @@ PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
            "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_obj_read", "slak_obj_write",
-           "slak_obj_free", "slak_plan_create",
+           "slak_obj_free", "slak_plan_create", "slak_plan_create_creased", "slak_subdivide_creased",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
@@ -88,6 +90,8 @@ def lib():
         L.slak_workspace_release.restype = I
         L.slak_subdivide_level_noalloc.argtypes = [P, P, I, V]
         L.slak_plan_create.argtypes = [P, I, I, I, V, ctypes.POINTER(V)]
+        L.slak_plan_create_creased.argtypes = [P, I, I, I, V, V, I64, V, ctypes.POINTER(V)]
+        L.slak_subdivide_creased.argtypes = [P, P, I, I, V, V, I64, V]
         L.slak_plan_execute.argtypes = [V, V]
         L.slak_plan_status.argtypes = [V, V]
         L.slak_plan_output.argtypes = [V, P]
@@ -114,7 +118,8 @@ def lib():
         for n in ("slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
                   "slak_batch_num_waves", "slak_batch_destroy"):
             getattr(L, n).restype = I
-        for n in ("slak_subdivide", "slak_mesh_free", "slak_subdivide_level_noalloc", "slak_plan_create", "slak_plan_execute", "slak_plan_status",
+        for n in ("slak_subdivide", "slak_mesh_free", "slak_subdivide_level_noalloc", "slak_plan_create",
+                  "slak_plan_create_creased", "slak_subdivide_creased", "slak_plan_execute", "slak_plan_status",
                   "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
                   "slak_plan_level_stats", "slak_plan_destroy"):
             getattr(L, n).restype = I

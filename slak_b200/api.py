@@ -155,16 +155,40 @@ class LAKCatmullClark(_Scheme):
     MeshInfo = DeviceMesh
 
 
+def _crease_tensors(creases):
+    """(pairs, sharpness) as contiguous int32 (m, 2) and float32 (m,) CUDA tensors."""
+    torch = _torch()
+    pairs, sharp = creases
+    pairs = torch.as_tensor(np.asarray(pairs) if not torch.is_tensor(pairs) else pairs)
+    sharp = torch.as_tensor(np.asarray(sharp) if not torch.is_tensor(sharp) else sharp)
+    pairs = pairs.to(device="cuda", dtype=torch.int32).reshape(-1, 2).contiguous()
+    sharp = sharp.to(device="cuda", dtype=torch.float32).reshape(-1).contiguous()
+    if pairs.shape[0] != sharp.shape[0]:
+        raise ValueError("creases: one sharpness per vertex pair")
+    return pairs, sharp
+
+
 class Plan:
     """Sized-once execution of ``levels`` subdivision levels (see slak_plan_create)."""
 
-    def __init__(self, cmesh: DeviceMesh, levels: int, scheme: int, flags: int = 0, stream=None):
+    def __init__(self, cmesh: DeviceMesh, levels: int, scheme: int, flags: int = 0, stream=None, creases=None):
+        """``creases``: None, or (pairs, sharpness) -- an (m, 2) array of vertex
+        ids and m sharpness values, host arrays or device tensors
+        (slak_plan_create_creased; the plan keeps its own copy)."""
         self._cmesh = cmesh            # the plan reads these arrays on every execute
         self._cin = cmesh.as_c()
         h = ctypes.c_void_p()
-        rc = _abi.lib().slak_plan_create(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
-                                         _stream_handle(stream), ctypes.byref(h))
-        _abi.check(rc, "slak_plan_create")
+        if creases is None:
+            rc = _abi.lib().slak_plan_create(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
+                                             _stream_handle(stream), ctypes.byref(h))
+            _abi.check(rc, "slak_plan_create")
+        else:
+            pairs, sharp = _crease_tensors(creases)
+            rc = _abi.lib().slak_plan_create_creased(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
+                                                     pairs.data_ptr() if pairs.numel() else None,
+                                                     sharp.data_ptr() if sharp.numel() else None,
+                                                     int(sharp.numel()), _stream_handle(stream), ctypes.byref(h))
+            _abi.check(rc, "slak_plan_create_creased")
         self._h = h
         self.scheme = scheme
 
@@ -227,11 +251,12 @@ class Plan:
             pass
 
 
-def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0) -> HostResult:
-    """Host mesh in, host refined mesh out (H2D, one plan execution, D2H)."""
+def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0, creases=None) -> HostResult:
+    """Host mesh in, host refined mesh out (H2D, one plan execution, D2H).
+    ``creases``: None or (pairs, sharpness), see Plan."""
     torch = _torch()
     dm = DeviceMesh.from_host(mesh)
-    plan = Plan(dm, levels, scheme, flags)
+    plan = Plan(dm, levels, scheme, flags, creases=creases)
     plan.execute()
     plan.check()
     out = plan.output().to_host()

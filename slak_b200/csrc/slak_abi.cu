@@ -26,6 +26,9 @@
 #include "general.cuh"
 #include "fast.cuh"
 #include "scan.cuh"
+#include "crease.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
 
 using namespace slak;
 
@@ -172,6 +175,21 @@ struct slak_plan {
     // per-launch timing (SLAK_PLAN_TIMING)
     std::vector<cudaEvent_t> ev;
     std::vector<KernelRec> recs;
+    // creases (slak_plan_create_creased): a snapshot of the pairs and
+    // sharpness, the crease list of each level that has a live crease
+    // (ncrease << level entries), the incidence records and their sort
+    int64_t ncrease = 0;
+    int crease_levels = 0;           // ceil(largest sharpness), at most the level count
+    int* c_pairs = nullptr;
+    float* c_sharp = nullptr;
+    int* c_mark = nullptr;           // level-0 corners already named by a crease
+    unsigned char* c_bnd0 = nullptr; // base vertices on the boundary (open meshes)
+    std::vector<int*> c_cc;
+    std::vector<float*> c_cs;
+    unsigned long long *c_kin = nullptr, *c_kout = nullptr;
+    int *c_vin = nullptr, *c_vout = nullptr;
+    void* c_tmp = nullptr;
+    size_t c_tmp_bytes = 0;
 };
 
 namespace {
@@ -386,6 +404,51 @@ void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, 
     }
 }
 
+// The crease pass of level li (after the level's own kernels): level 0 first
+// resolves the crease pairs on its vertex columns.
+void launch_creases(slak_plan* p, int li, Lc& lc)
+{
+    const Level& L = p->lv[li];
+    const Level& L0 = p->lv[0];
+    cudaStream_t str = lc.s;
+    const int64_t n = p->ncrease << li;
+    if (li == 0) {
+        cudaMemsetAsync(p->c_mark, 0, sizeof(int) * (size_t)L0.N, str);
+        k_crease_resolve<<<grid_for(p->ncrease), kBlock, 0, str>>>(p->c_pairs, p->c_sharp, (int)p->ncrease,
+                                                                   (int)L0.V, p->s.sptr, p->s.sc, p->s.snext,
+                                                                   p->c_mark, p->c_cc[0], p->c_cs[0], p->st);
+        lc.after("k_crease_resolve");
+        if (p->c_bnd0) {
+            k_crease_bnd0<<<grid_for(L0.V), kBlock, 0, str>>>((int)L0.V, p->s.sptr, p->s.sflag, SF_BOUT | SF_BIN,
+                                                              p->c_bnd0);
+            lc.after("k_crease_bnd0");
+        }
+    }
+    const bool more = li + 1 < p->crease_levels;
+    int* ncc = more ? p->c_cc[li + 1] : nullptr;
+    float* ncs = more ? p->c_cs[li + 1] : nullptr;
+    if (L.quad)
+        k_crease_edges<true><<<grid_for(n), kBlock, 0, str>>>(Faces<true>{nullptr, nullptr}, L.ids, L.o_ids, L.verts,
+                                                               L.o_verts, p->c_cc[li], p->c_cs[li], (int)n, p->c_kin,
+                                                               p->c_vin, ncc, ncs);
+    else
+        k_crease_edges<false><<<grid_for(n), kBlock, 0, str>>>(Faces<false>{L.ptr, p->s.cface}, L.ids, L.o_ids,
+                                                                L.verts, L.o_verts, p->c_cc[li], p->c_cs[li], (int)n,
+                                                                p->c_kin, p->c_vin, ncc, ncs);
+    lc.after("k_crease_edges");
+    size_t tb = p->c_tmp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(p->c_tmp, tb, p->c_kin, p->c_kout, p->c_vin, p->c_vout,
+                                                    (int)(2 * n), 0, 64, str);
+    if (e != cudaSuccess && !lc.err) {
+        lc.err = cuda_status(e);
+        g_detail = std::string("crease sort: ") + cudaGetErrorString(e);
+    }
+    lc.after("sort(creases)");
+    k_crease_verts<<<grid_for(2 * n), kBlock, 0, str>>>(p->c_kout, p->c_vout, (int)(2 * n), p->c_cs[li], p->c_bnd0,
+                                                        (int)L0.V, L.verts, L.o_verts);
+    lc.after("k_crease_verts");
+}
+
 int enqueue_all(slak_plan* p, cudaStream_t str)
 {
     int64_t nl = 0;
@@ -407,6 +470,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         lc.level = (int)li;
         if (L.fast) {
             launch_fast(p->lv[li - 1], L, p->s.cface, p->scheme, comp, lc);
+            if ((int)li < p->crease_levels) launch_creases(p, (int)li, lc);
             continue;
         }
         launch_topology_a(L, (int)li, p->scheme, p->s, p->st, lc);
@@ -431,6 +495,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
             scan_exclusive(p->s.xisb, p->s.xbrank, L.E, p->s.tmp, str, &n3);
             lc.after("scan(boundary)", (int)n3);
         }
+        if ((int)li < p->crease_levels) launch_creases(p, (int)li, lc);
     }
     p->launches = nl;
     if (lc.err) return lc.err;
@@ -611,6 +676,24 @@ void plan_carve(slak_plan* p, Carver& cv)
         p->ping_verts[k] = nlev > 1 ? cv.take<float>(4 * p->mid_verts) : nullptr;
     }
     p->st = cv.take<DevStatus>(1);
+    if (p->crease_levels > 0) {
+        const int64_t m = p->ncrease, nmax = m << (p->crease_levels - 1);
+        p->c_pairs = cv.take<int>(2 * m);
+        p->c_sharp = cv.take<float>(m);
+        p->c_mark = cv.take<int>(p->lv[0].N);
+        p->c_bnd0 = p->lv[0].B > 0 ? cv.take<unsigned char>(p->lv[0].V) : nullptr;
+        p->c_cc.assign(p->crease_levels, nullptr);
+        p->c_cs.assign(p->crease_levels, nullptr);
+        for (int l = 0; l < p->crease_levels; ++l) {
+            p->c_cc[l] = cv.take<int>(m << l);
+            p->c_cs[l] = cv.take<float>(m << l);
+        }
+        p->c_kin = cv.take<unsigned long long>(2 * nmax);
+        p->c_kout = cv.take<unsigned long long>(2 * nmax);
+        p->c_vin = cv.take<int>(2 * nmax);
+        p->c_vout = cv.take<int>(2 * nmax);
+        p->c_tmp = cv.take<char>((int64_t)p->c_tmp_bytes);
+    }
 }
 
 // Counts and flags of the refined mesh (arrays not set).
@@ -846,8 +929,37 @@ int plan_autotune(slak_plan* p, cudaStream_t str)
 
 // Plan creation; with `ws`, the arena and the status word come from the
 // workspace (the plan does not own them).
+// Crease list sizing from a host copy of the sharpness (one sync): levels with
+// a live crease, and the sort's scratch.
+static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, cudaStream_t str)
+{
+    std::vector<float> h((size_t)m);
+    cudaError_t e = cudaMemcpyAsync(h.data(), sharp, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, str);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(str);
+    if (e != cudaSuccess) { g_detail = std::string("crease sharpness: ") + cudaGetErrorString(e); return cuda_status(e); }
+    float smax = 0.0f;
+    for (float x : h) {
+        if (!std::isfinite(x)) { g_detail = "crease sharpness is not finite"; return SLAK_ERR_INVALID_ARG; }
+        smax = std::max(smax, x);
+    }
+    const int nlev = (int)p->lv.size();
+    int cl = smax > 0.0f ? (int)std::ceil((double)smax) : 0;
+    p->ncrease = m;
+    p->crease_levels = std::min(cl, nlev);
+    if (p->crease_levels == 0) return SLAK_OK;
+    if ((m << p->crease_levels) >= (1ll << 30)) return SLAK_ERR_UNSUPPORTED;
+    const int n2 = (int)(2 * (m << (p->crease_levels - 1)));
+    size_t tb = 0;
+    e = cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (int*)nullptr, (int*)nullptr, n2, 0, 64, str);
+    if (e != cudaSuccess) return cuda_status(e);
+    p->c_tmp_bytes = tb;
+    return SLAK_OK;
+}
+
 static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, int flags, cudaStream_t str,
-                            Workspace* ws, slak_plan** out_plan)
+                            Workspace* ws, slak_plan** out_plan, const int* cpairs = nullptr,
+                            const float* csharp = nullptr, int64_t ncrease = 0)
 {
     *out_plan = nullptr;
     int rc = validate_mesh(cm, scheme);
@@ -868,6 +980,7 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
     }
     rc = probe_level0(p, p->lv[0], str, probe_mem);
     if (rc == SLAK_OK) rc = plan_levels(p);
+    if (rc == SLAK_OK && ncrease > 0) rc = plan_crease_setup(p, csharp, ncrease, str);
     if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
     Carver dry(nullptr);
     plan_carve(p, dry);
@@ -890,6 +1003,12 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
         if (ce == cudaSuccess) ce = cudaMalloc(&o.vals, sizeof(int) * (size_t)o.nnz);
     }
     p->out = o;
+    if (ce == cudaSuccess && p->crease_levels > 0) {   // the plan keeps its own copy of the creases
+        ce = cudaMemcpyAsync(p->c_pairs, cpairs, sizeof(int) * 2 * (size_t)ncrease, cudaMemcpyDeviceToDevice, str);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(p->c_sharp, csharp, sizeof(float) * (size_t)ncrease, cudaMemcpyDeviceToDevice, str);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(str);
+    }
     if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
     plan_wire(p);
     if (flags & SLAK_PLAN_AUTOTUNE) rc = plan_autotune(p, str);
@@ -926,6 +1045,33 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
     if (!cm || !out_plan) return SLAK_ERR_INVALID_ARG;
     return plan_create_impl(cm, target_level, scheme, flags, reinterpret_cast<cudaStream_t>(stream), nullptr,
                             out_plan);
+}
+
+int slak_plan_create_creased(const slak_mesh* cm, int target_level, int scheme, int flags,
+                             const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                             slak_stream_t stream, slak_plan** out_plan)
+{
+    if (!cm || !out_plan || ncreases < 0) return SLAK_ERR_INVALID_ARG;
+    if (ncreases > 0 && (!crease_verts || !crease_sharpness)) return SLAK_ERR_INVALID_ARG;
+    return plan_create_impl(cm, target_level, scheme, flags, reinterpret_cast<cudaStream_t>(stream), nullptr,
+                            out_plan, crease_verts, crease_sharpness, ncreases);
+}
+
+int slak_subdivide_creased(const slak_mesh* cm, slak_mesh* rm, int target_level, int scheme,
+                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                           slak_stream_t stream)
+{
+    if (!cm || !rm) return SLAK_ERR_INVALID_ARG;
+    std::memset(rm, 0, sizeof(*rm));
+    slak_plan* p = nullptr;
+    int rc = slak_plan_create_creased(cm, target_level, scheme, 0, crease_verts, crease_sharpness, ncreases, stream,
+                                      &p);
+    if (rc != SLAK_OK) return rc;
+    rc = slak_plan_execute(p, stream);
+    if (rc == SLAK_OK) rc = slak_plan_status(p, stream);
+    if (rc == SLAK_OK) rc = slak_plan_release_output(p, rm);
+    slak_plan_destroy(p);
+    return rc;
 }
 
 int slak_plan_execute(slak_plan* p, slak_stream_t stream)
