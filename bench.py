@@ -127,15 +127,23 @@ def _workload(name):
     return w.mesh, w.levels
 
 
-def cpu_baseline(mesh, levels, scheme, budget_s=20.0, single_budget_s=10.0):
+def cpu_baseline(mesh, levels, scheme, budget_s=20.0, single_budget_s=10.0, creases=None):
     """The oracle (CPU restatement, OpenMP) on the largest prefix of levels that
     fits the budget; refined faces of that sample per second.  A single-thread
-    figure of the same restatement rides along under "single_thread"."""
+    figure of the same restatement rides along under "single_thread".  With
+    creases, the oracle levels plus the numpy crease restatement."""
     import oracle
+    from oracle import creases as oc
+
+    def run(lv):
+        if creases is None:
+            return oracle.subdivide(mesh, lv, scheme)
+        return oc.subdivide_creased(mesh, lv, scheme, *creases)
+
     best = None
     for lv in range(1, levels + 1):
         t0 = time.perf_counter()
-        r = oracle.subdivide(mesh, lv, scheme)
+        r = run(lv)
         dt = time.perf_counter() - t0
         best = (lv, r.nfaces, dt)
         if dt * 4.5 > budget_s:
@@ -150,7 +158,7 @@ def cpu_baseline(mesh, levels, scheme, budget_s=20.0, single_budget_s=10.0):
             one = None
             for l1 in range(1, levels + 1):
                 t0 = time.perf_counter()
-                r = oracle.subdivide(mesh, l1, scheme)
+                r = run(l1)
                 d1 = time.perf_counter() - t0
                 one = (l1, r.nfaces, d1)
                 if d1 * 4.5 > single_budget_s:
@@ -161,6 +169,23 @@ def cpu_baseline(mesh, levels, scheme, budget_s=20.0, single_budget_s=10.0):
         out["single_thread"] = {"value": f1 / d1, "unit": "refined_faces/s", "cores": 1,
                                 "sample": f"{l1} of {levels} levels ({f1} refined faces) in {d1:.2f} s"}
     return out
+
+
+def _creases(mesh, frac, seed=11):
+    """A seeded fraction of the mesh's edges as creases, sharpness drawn from
+    {0.5, 1, 2, 3, 5} (live for up to five levels); None when frac <= 0."""
+    if frac <= 0:
+        return None
+    ptr = mesh.ptr if mesh.ptr is not None else np.arange(mesh.nfaces + 1) * 4
+    ids = np.asarray(mesh.ids, np.int64)
+    c = np.arange(ids.size)
+    face = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    nxt = np.where(c + 1 == np.asarray(ptr)[face + 1], np.asarray(ptr)[face], c + 1)
+    e = np.unique(np.sort(np.stack([ids, ids[nxt]], 1), 1), axis=0)
+    rng = np.random.default_rng(seed)
+    pick = e[rng.random(e.shape[0]) < frac].astype(np.int32)
+    sharp = rng.choice(np.array([0.5, 1.0, 2.0, 3.0, 5.0], np.float32), pick.shape[0])
+    return pick, sharp
 
 
 def run_ours(args, dist, rank, ws):
@@ -175,8 +200,9 @@ def run_ours(args, dist, rank, ws):
     stream = torch.cuda.Stream()
     dm = api.DeviceMesh.from_host(mesh)
     flags = api._abi.PLAN_GRAPH | (0 if args.no_tune else api._abi.PLAN_AUTOTUNE)
+    creases = _creases(mesh, args.crease_frac)
     with torch.cuda.stream(stream):
-        plan = api.Plan(dm, levels, scheme, flags, stream=stream)     # tuning runs here, untimed
+        plan = api.Plan(dm, levels, scheme, flags, stream=stream, creases=creases)   # tuning runs here, untimed
     stats = plan.level_stats()
     tuning = []
     for t in plan.tuning():
@@ -213,7 +239,7 @@ def run_ours(args, dist, rank, ws):
     launches = plan.launches * args.steps
 
     # dominant kernel: per-kernel events of instrumented eager executions
-    kern, ktable = plan_kernel_profile(dm, levels, scheme, args.steps, stream, torch, flush)
+    kern, ktable = plan_kernel_profile(dm, levels, scheme, args.steps, stream, torch, flush, creases)
     tpu = TRAFFIC_PER_UNIT.get((kern["kernel"], args.scheme, "last" if kern["level"] == levels - 1 else "mid"))
     if tpu is not None:
         units = stats[kern["level"]]["nfaces"]
@@ -233,7 +259,7 @@ def run_ours(args, dist, rank, ws):
                           "frac": (b / (ms_l * 1e-3) / 1e9) / peak if ms_l > 0 else None})
 
     # e2e: host buffers, the C-ABI drop-in call
-    e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws)
+    e2e = run_e2e(mesh, levels, scheme, args, torch, dist, ws, creases)
 
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_step * 1e-3) / 1e9
@@ -244,7 +270,9 @@ def run_ours(args, dist, rank, ws):
         "config": {"workload": f"{args.workload}: {mesh.nfaces} faces, {mesh.nverts} verts, {args.scheme.upper()}, "
                                f"{levels} levels -> {faces} quads", "scheme": args.scheme.upper(),
                    "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
-                   "parallelism": f"replicas x{ws}"},
+                   "parallelism": f"replicas x{ws}",
+                   **({"creases": f"{creases[1].size} crease edges ({args.crease_frac:g} of the edges), "
+                                  f"sharpness in {{0.5, 1, 2, 3, 5}}"} if creases is not None else {})},
         "gpu_launches": launches,
         "ms_per_step_spread": spread,
         "roofline": kern,
@@ -259,12 +287,12 @@ def run_ours(args, dist, rank, ws):
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(mesh, levels, scheme, args.cpu_budget)
+        out["cpu_baseline"] = cpu_baseline(mesh, levels, scheme, args.cpu_budget, creases=creases)
     plan.close()
     return out
 
 
-def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush):
+def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush, creases=None):
     """Per-kernel device times from CUDA events recorded after every launch of an
     eager execution (SLAK_PLAN_TIMING), averaged over `steps` timed executions
     with the L2 flushed before each; returns the dominant kernel's roofline and
@@ -272,7 +300,7 @@ def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush):
     from slak_b200 import api
     peak, peak_kind = _peaks()
     with torch.cuda.stream(stream):
-        plan = api.Plan(dm, levels, scheme, api._abi.PLAN_TIMING, stream=stream)
+        plan = api.Plan(dm, levels, scheme, api._abi.PLAN_TIMING, stream=stream, creases=creases)
         plan.execute(stream)
         plan.check(stream)
         acc = {}
@@ -304,7 +332,7 @@ def plan_kernel_profile(dm, levels, scheme, steps, stream, torch, flush):
     return roof, sorted(table, key=lambda t: -t["ms"])
 
 
-def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
+def run_e2e(mesh, levels, scheme, args, torch, dist, ws, creases=None):
     import ctypes
     from slak_b200 import _abi, api
     lib = _abi.lib()
@@ -324,17 +352,26 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws):
     sh = int(stream.cuda_stream) or None
     out_ids = out_verts = None
     times = []
-    h2d = sum(t.numel() * t.element_size() for t in (h_ptr, h_ids, h_vals, h_verts) if t is not None)
+    h_cp = pin(creases[0].reshape(-1)) if creases is not None else None
+    h_cs = pin(creases[1]) if creases is not None else None
+    d_cp = torch.empty_like(h_cp, device="cuda") if h_cp is not None else None
+    d_cs = torch.empty_like(h_cs, device="cuda") if h_cs is not None else None
+    h2d = sum(t.numel() * t.element_size() for t in (h_ptr, h_ids, h_vals, h_verts, h_cp, h_cs) if t is not None)
     d2h = 0
     n = max(2, min(args.steps, 5))
     for i in range(args.warmup + n):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for h, d in ((h_ptr, d_ptr), (h_ids, d_ids), (h_vals, d_vals), (h_verts, d_verts)):
+        for h, d in ((h_ptr, d_ptr), (h_ids, d_ids), (h_vals, d_vals), (h_verts, d_verts), (h_cp, d_cp),
+                     (h_cs, d_cs)):
             if h is not None:
                 d.copy_(h, non_blocking=True)
         cout = _abi.SlakMesh()
-        rc = lib.slak_subdivide(ctypes.byref(cin), ctypes.byref(cout), levels, scheme, sh)
+        if creases is None:
+            rc = lib.slak_subdivide(ctypes.byref(cin), ctypes.byref(cout), levels, scheme, sh)
+        else:
+            rc = lib.slak_subdivide_creased(ctypes.byref(cin), ctypes.byref(cout), levels, scheme, d_cp.data_ptr(),
+                                            d_cs.data_ptr(), int(h_cs.numel()), sh)
         _abi.check(rc, "slak_subdivide")
         if out_ids is None:
             out_ids = torch.empty(cout.nnz, dtype=torch.int32).pin_memory()
@@ -538,6 +575,9 @@ def run_reference(args, dist, rank, ws):
     scheme = SLAK if args.scheme == "slak" else LAK
     if not ref.available():
         return {"impl": "reference", "unavailable": "reference library oracle/_ref/libslak_ref.so not built"}
+    if args.crease_frac > 0:
+        return {"impl": "reference", "unavailable": "the reference does not implement creases "
+                                                    "(handleCreases is commented out, CatmullClarkImpl.cu:94-96)"}
     if args.workload == "batch2000":
         return run_reference_batch(args, scheme)
     mesh, levels = _workload(args.workload)
@@ -586,6 +626,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuning)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--crease-frac", type=float, default=0.0,
+                    help="refine with this seeded fraction of the edges as semi-sharp creases")
     ap.add_argument("--batch-count", type=int, default=2000)
     ap.add_argument("--batch-plain-reps", type=int, default=1)
     args = ap.parse_args()

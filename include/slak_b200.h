@@ -109,6 +109,27 @@ int slak_obj_read(const char* path, slak_mesh* out);
 int slak_obj_write(const char* path, const slak_mesh* host_mesh);
 int slak_obj_free(slak_mesh* host_mesh);
 
+/* Crease pairs of a mesh (host or device memory, as the call says):
+ * 2 * count vertex ids and count sharpness values. */
+typedef struct slak_creases {
+    int64_t count;
+    int32_t* verts;
+    float* sharpness;
+} slak_creases;
+
+/* As slak_obj_read, and also turns the file's "t crease" tags into host
+ * crease pairs (malloc; release with slak_obj_free_creases).  OBJ::read keeps
+ * every "t <type> <ni>/<nf>/<ns> ints... floats..." line as a Tag
+ * (include/obj.h:92-99, 202-229) that the reference never uses.  Here a
+ * crease tag's ni >= 2 ints are a chain of 0-based vertex ids (edges
+ * {v_j, v_j+1}) with one sharpness (nf == 1) or one per edge (nf == ni - 1);
+ * other tag types are skipped; a malformed crease tag or an id out of range
+ * gives SLAK_ERR_BAD_MESH.  slak_obj_write_creased appends one
+ * "t crease 2/1/0 a b s" line per pair. */
+int slak_obj_read_creased(const char* path, slak_mesh* out, slak_creases* creases);
+int slak_obj_write_creased(const char* path, const slak_mesh* host_mesh, const slak_creases* creases);
+int slak_obj_free_creases(slak_creases* creases);
+
 /* Frees the current device's cached slak_subdivide workspace.  No counterpart
  * in the reference, whose calls keep nothing between them.  Returns
  * SLAK_ERR_NOT_READY while a call holds the workspace. */

@@ -21,12 +21,18 @@ PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
            "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_obj_read", "slak_obj_write",
-           "slak_obj_free", "slak_plan_create", "slak_plan_create_creased", "slak_subdivide_creased",
+           "slak_obj_free", "slak_obj_read_creased", "slak_obj_write_creased", "slak_obj_free_creases",
+           "slak_plan_create", "slak_plan_create_creased", "slak_subdivide_creased",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
            "slak_plan_destroy", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
            "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
+
+
+class SlakCreases(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int64), ("verts", ctypes.POINTER(ctypes.c_int32)),
+                ("sharpness", ctypes.POINTER(ctypes.c_float))]
 
 
 class SlakMesh(ctypes.Structure):
@@ -84,7 +90,12 @@ def lib():
         L.slak_obj_read.argtypes = [ctypes.c_char_p, P]
         L.slak_obj_write.argtypes = [ctypes.c_char_p, P]
         L.slak_obj_free.argtypes = [P]
-        for n in ("slak_obj_read", "slak_obj_write", "slak_obj_free"):
+        PC = ctypes.POINTER(SlakCreases)
+        L.slak_obj_read_creased.argtypes = [ctypes.c_char_p, P, PC]
+        L.slak_obj_write_creased.argtypes = [ctypes.c_char_p, P, PC]
+        L.slak_obj_free_creases.argtypes = [PC]
+        for n in ("slak_obj_read", "slak_obj_write", "slak_obj_free", "slak_obj_read_creased", "slak_obj_write_creased",
+                  "slak_obj_free_creases"):
             getattr(L, n).restype = I
         L.slak_workspace_release.argtypes = []
         L.slak_workspace_release.restype = I

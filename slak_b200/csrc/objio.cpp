@@ -9,6 +9,14 @@
 // each: a first pass counts each chunk's "v" lines, so a chunk knows how many
 // vertices precede it and can resolve negative indices; a second pass parses.
 // Writing formats chunks of lines in parallel and writes them in order.
+//
+// Crease tags.  OBJ::read keeps every "t" line as a Tag {type, intargs,
+// floatargs} (include/obj.h:92-99, 202-229: "t <type> <ni>/<nf>/<ns>" then ni
+// ints and nf floats); the reference never uses them.  slak_obj_read_creased
+// turns "t crease" tags into crease pairs: the ni >= 2 ints are a chain of
+// 0-based vertex ids v0 v1 ... (edges {v_j, v_j+1}), with one sharpness for
+// the whole chain (nf == 1) or one per edge (nf == ni - 1).  Other tag types
+// are skipped.
 #include "slak_b200.h"
 
 #include <algorithm>
@@ -30,7 +38,9 @@ struct Chunk {
     std::vector<float> v;      // x, y, z per vertex
     std::vector<int32_t> fo;   // face sizes
     std::vector<int32_t> fi;   // corner vertex indices, 0-based
-    int err_line = 0;          // nonzero: 1-based line (within the chunk) of a malformed face
+    std::vector<int32_t> cv;   // crease pairs (2 ids each), when tags are read
+    std::vector<float> cs;     // their sharpness
+    int err_line = 0;          // nonzero: 1-based line (within the chunk) of a malformed face or tag
     int64_t lines = 0;
 };
 
@@ -48,6 +58,54 @@ inline const char* line_end(const char* p, const char* e)
 
 inline bool is_v(const char* p, const char* le) { return le - p >= 2 && p[0] == 'v' && (p[1] == ' ' || p[1] == '\t'); }
 inline bool is_f(const char* p, const char* le) { return le - p >= 2 && p[0] == 'f' && (p[1] == ' ' || p[1] == '\t'); }
+inline bool is_t(const char* p, const char* le) { return le - p >= 2 && p[0] == 't' && (p[1] == ' ' || p[1] == '\t'); }
+
+// One "t" line (after the "t"): appends a crease tag's edges; false if malformed.
+bool parse_tag(const char* q, const char* le, Chunk& c)
+{
+    std::string line(q, le);
+    const char* p = line.c_str();
+    const char* e = p + line.size();
+    p = skip_ws(p, e);
+    const char* tb = p;
+    while (p < e && *p != ' ' && *p != '\t' && *p != '\r') ++p;
+    const std::string type(tb, p);
+    char* end = nullptr;
+    long n[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+        p = skip_ws(p, e);
+        n[k] = std::strtol(p, &end, 10);
+        if (end == p || n[k] < 0) return false;
+        p = end;
+        if (k < 2) {
+            if (p >= e || *p != '/') return false;
+            ++p;
+        }
+    }
+    if (type != "crease") return true;
+    const long ni = n[0], nf = n[1];
+    if (ni < 2 || (nf != 1 && nf != ni - 1)) return false;
+    std::vector<long> v((size_t)ni);
+    for (long k = 0; k < ni; ++k) {
+        p = skip_ws(p, e);
+        v[(size_t)k] = std::strtol(p, &end, 10);
+        if (end == p || v[(size_t)k] < 0 || v[(size_t)k] > INT32_MAX) return false;
+        p = end;
+    }
+    std::vector<float> f((size_t)nf);
+    for (long k = 0; k < nf; ++k) {
+        p = skip_ws(p, e);
+        f[(size_t)k] = std::strtof(p, &end);
+        if (end == p) return false;
+        p = end;
+    }
+    for (long k = 0; k + 1 < ni; ++k) {
+        c.cv.push_back((int32_t)v[(size_t)k]);
+        c.cv.push_back((int32_t)v[(size_t)k + 1]);
+        c.cs.push_back(nf == 1 ? f[0] : f[(size_t)k]);
+    }
+    return true;
+}
 
 void count_pass(Chunk& c)
 {
@@ -59,8 +117,8 @@ void count_pass(Chunk& c)
     }
 }
 
-// base: vertices defined before this chunk
-void parse_pass(Chunk& c, int64_t base)
+// base: vertices defined before this chunk; tags: read "t crease" lines
+void parse_pass(Chunk& c, int64_t base, bool tags)
 {
     int64_t nv = base;
     std::string tmp;
@@ -98,6 +156,8 @@ void parse_pass(Chunk& c, int64_t base)
             }
             if (c.err_line) break;
             c.fo.push_back(order);
+        } else if (tags && is_t(s, le)) {
+            if (!parse_tag(s + 1, le, c)) { c.err_line = (int)c.lines; break; }
         }
         p = le + 1;
     }
@@ -110,14 +170,11 @@ int nthreads_for(size_t bytes)
     return (int)std::max<size_t>(1, std::min<size_t>(hc ? hc : 1, by_size));
 }
 
-}  // namespace
-
-extern "C" {
-
-int slak_obj_read(const char* path, slak_mesh* out)
+int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
 {
     if (!path || !out) return SLAK_ERR_INVALID_ARG;
     std::memset(out, 0, sizeof(*out));
+    if (cr) std::memset(cr, 0, sizeof(*cr));
     FILE* f = std::fopen(path, "rb");
     if (!f) return SLAK_ERR_INVALID_ARG;
     std::fseek(f, 0, SEEK_END);
@@ -153,7 +210,7 @@ int slak_obj_read(const char* path, slak_mesh* out)
     run([&](int t) { count_pass(ch[t]); });
     std::vector<int64_t> vbase(nt + 1, 0);
     for (int t = 0; t < nt; ++t) vbase[t + 1] = vbase[t] + ch[t].nv;
-    run([&](int t) { parse_pass(ch[t], vbase[t]); });
+    run([&](int t) { parse_pass(ch[t], vbase[t], cr != nullptr); });
 
     int64_t F = 0, N = 0, V = vbase[nt];
     for (auto& c : ch) {
@@ -195,9 +252,36 @@ int slak_obj_read(const char* path, slak_mesh* out)
     });
     ptr[F] = (int32_t)N;
     for (int64_t c = 0; c < N && !bad; ++c) bad = ids[c] >= V;
+    int64_t C = 0;
+    for (auto& c : ch) {
+        C += (int64_t)c.cs.size();
+        for (int32_t x : c.cv) bad |= x >= V;
+    }
+    int32_t* cverts = nullptr;
+    float* csharp = nullptr;
+    if (!bad && cr && C > 0) {
+        cverts = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * 2 * (size_t)C));
+        csharp = static_cast<float*>(std::malloc(sizeof(float) * (size_t)C));
+        if (!cverts || !csharp) {
+            std::free(cverts); std::free(csharp);
+            std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
+            return SLAK_ERR_OOM;
+        }
+        int64_t o = 0;
+        for (auto& c : ch) {
+            std::memcpy(cverts + 2 * o, c.cv.data(), sizeof(int32_t) * c.cv.size());
+            std::memcpy(csharp + o, c.cs.data(), sizeof(float) * c.cs.size());
+            o += (int64_t)c.cs.size();
+        }
+    }
     if (bad) {
         std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
         return SLAK_ERR_BAD_MESH;
+    }
+    if (cr) {
+        cr->count = C;
+        cr->verts = cverts;
+        cr->sharpness = csharp;
     }
     out->type = (F > 0 && min_order == 3 && max_order == 3) ? SLAK_MESH_TRI
               : (F > 0 && min_order == 4 && max_order == 4) ? SLAK_MESH_QUAD : SLAK_MESH_POLY;
@@ -213,8 +297,10 @@ int slak_obj_read(const char* path, slak_mesh* out)
     return SLAK_OK;
 }
 
-int slak_obj_write(const char* path, const slak_mesh* m)
+int obj_write(const char* path, const slak_mesh* m, const slak_creases* cr)
 {
+    if (cr && cr->count < 0) return SLAK_ERR_INVALID_ARG;
+    if (cr && cr->count > 0 && (!cr->verts || !cr->sharpness)) return SLAK_ERR_INVALID_ARG;
     if (!path || !m || m->nverts < 0 || m->nfaces < 0 || (m->nverts > 0 && !m->verts)) return SLAK_ERR_INVALID_ARG;
     const int fixed = m->type == SLAK_MESH_QUAD ? 4 : m->type == SLAK_MESH_TRI ? 3 : 0;
     if (m->nfaces > 0 && (!m->ids || (!fixed && !m->ptr))) return SLAK_ERR_INVALID_ARG;
@@ -260,8 +346,45 @@ int slak_obj_write(const char* path, const slak_mesh* m)
     bool ok = true;
     for (auto& s : part) ok &= std::fwrite(s.data(), 1, s.size(), f) == s.size();
     for (auto& s : fpart) ok &= std::fwrite(s.data(), 1, s.size(), f) == s.size();
+    if (cr) {
+        char line[96];
+        for (int64_t k = 0; k < cr->count && ok; ++k) {
+            const int n = std::snprintf(line, sizeof line, "t crease 2/1/0 %d %d %.9g\n", cr->verts[2 * k],
+                                        cr->verts[2 * k + 1], cr->sharpness[k]);
+            ok &= std::fwrite(line, 1, (size_t)n, f) == (size_t)n;
+        }
+    }
     ok &= std::fclose(f) == 0;
     return ok ? SLAK_OK : SLAK_ERR_INVALID_ARG;
+}
+
+}  // namespace
+
+extern "C" {
+
+int slak_obj_read(const char* path, slak_mesh* out) { return obj_read(path, out, nullptr); }
+
+int slak_obj_read_creased(const char* path, slak_mesh* out, slak_creases* creases)
+{
+    if (!creases) return SLAK_ERR_INVALID_ARG;
+    return obj_read(path, out, creases);
+}
+
+int slak_obj_write(const char* path, const slak_mesh* m) { return obj_write(path, m, nullptr); }
+
+int slak_obj_write_creased(const char* path, const slak_mesh* m, const slak_creases* creases)
+{
+    if (!creases) return SLAK_ERR_INVALID_ARG;
+    return obj_write(path, m, creases);
+}
+
+int slak_obj_free_creases(slak_creases* c)
+{
+    if (!c) return SLAK_ERR_INVALID_ARG;
+    std::free(c->verts);
+    std::free(c->sharpness);
+    std::memset(c, 0, sizeof(*c));
+    return SLAK_OK;
 }
 
 int slak_obj_free(slak_mesh* m)

@@ -28,8 +28,6 @@
 #include "scan.cuh"
 #include "crease.cuh"
 
-#include <cub/device/device_radix_sort.cuh>
-
 using namespace slak;
 
 namespace {
@@ -177,19 +175,18 @@ struct slak_plan {
     std::vector<KernelRec> recs;
     // creases (slak_plan_create_creased): a snapshot of the pairs and
     // sharpness, the crease list of each level that has a live crease
-    // (ncrease << level entries), the incidence records and their sort
+    // (ncrease << level entries), the base vertices' crease edges (CSR) and
+    // the edge points made on live creases
     int64_t ncrease = 0;
     int crease_levels = 0;           // ceil(largest sharpness), at most the level count
     int* c_pairs = nullptr;
     float* c_sharp = nullptr;
-    int* c_mark = nullptr;           // level-0 corners already named by a crease
+    int* c_mark = nullptr;           // level-0 corner -> live crease entry + 1
     unsigned char* c_bnd0 = nullptr; // base vertices on the boundary (open meshes)
+    int *c_vcnt = nullptr, *c_vptr = nullptr, *c_inc = nullptr;
     std::vector<int*> c_cc;
     std::vector<float*> c_cs;
-    unsigned long long *c_kin = nullptr, *c_kout = nullptr;
-    int *c_vin = nullptr, *c_vout = nullptr;
-    void* c_tmp = nullptr;
-    size_t c_tmp_bytes = 0;
+    std::vector<int*> c_ep;          // per level t < crease_levels - 1: edge point of entry j, or -1
 };
 
 namespace {
@@ -405,48 +402,53 @@ void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, 
 }
 
 // The crease pass of level li (after the level's own kernels): level 0 first
-// resolves the crease pairs on its vertex columns.
-void launch_creases(slak_plan* p, int li, Lc& lc)
+// resolves the crease pairs on its vertex columns and lists each base
+// vertex's crease edges.
+template <bool QUAD>
+void launch_creases_t(slak_plan* p, int li, Faces<QUAD> fc, Lc& lc)
 {
     const Level& L = p->lv[li];
     const Level& L0 = p->lv[0];
     cudaStream_t str = lc.s;
-    const int64_t n = p->ncrease << li;
+    const int64_t m = p->ncrease, n = m << li;
+    const int V0 = (int)L0.V;
     if (li == 0) {
         cudaMemsetAsync(p->c_mark, 0, sizeof(int) * (size_t)L0.N, str);
-        k_crease_resolve<<<grid_for(p->ncrease), kBlock, 0, str>>>(p->c_pairs, p->c_sharp, (int)p->ncrease,
-                                                                   (int)L0.V, p->s.sptr, p->s.sc, p->s.snext,
-                                                                   p->c_mark, p->c_cc[0], p->c_cs[0], p->st);
+        k_crease_resolve<<<grid_for(m), kBlock, 0, str>>>(p->c_pairs, p->c_sharp, (int)m, V0, p->s.sptr, p->s.sc,
+                                                          p->s.snext, p->c_mark, p->c_cc[0], p->c_cs[0], p->st);
         lc.after("k_crease_resolve");
-        if (p->c_bnd0) {
-            k_crease_bnd0<<<grid_for(L0.V), kBlock, 0, str>>>((int)L0.V, p->s.sptr, p->s.sflag, SF_BOUT | SF_BIN,
-                                                              p->c_bnd0);
-            lc.after("k_crease_bnd0");
-        }
+        k_crease_vinc<false><<<grid_for(V0), kBlock, 0, str>>>(V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
+                                                               SF_BOUT | SF_BIN, p->c_mark, p->c_vcnt, p->c_bnd0,
+                                                               nullptr, nullptr);
+        lc.after("k_crease_vinc");
+        int64_t ns = 0;
+        scan_exclusive(p->c_vcnt, p->c_vptr, V0, p->s.tmp, str, &ns);
+        lc.after("scan(crease vertices)", (int)ns);
+        k_crease_vinc<true><<<grid_for(V0), kBlock, 0, str>>>(V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
+                                                              SF_BOUT | SF_BIN, p->c_mark, nullptr, nullptr,
+                                                              p->c_vptr, p->c_inc);
+        lc.after("k_crease_vinc");
     }
     const bool more = li + 1 < p->crease_levels;
-    int* ncc = more ? p->c_cc[li + 1] : nullptr;
-    float* ncs = more ? p->c_cs[li + 1] : nullptr;
-    if (L.quad)
-        k_crease_edges<true><<<grid_for(n), kBlock, 0, str>>>(Faces<true>{nullptr, nullptr}, L.ids, L.o_ids, L.verts,
-                                                               L.o_verts, p->c_cc[li], p->c_cs[li], (int)n, p->c_kin,
-                                                               p->c_vin, ncc, ncs);
-    else
-        k_crease_edges<false><<<grid_for(n), kBlock, 0, str>>>(Faces<false>{L.ptr, p->s.cface}, L.ids, L.o_ids,
-                                                                L.verts, L.o_verts, p->c_cc[li], p->c_cs[li], (int)n,
-                                                                p->c_kin, p->c_vin, ncc, ncs);
+    k_crease_edges<QUAD><<<grid_for(n), kBlock, 0, str>>>(fc, L.ids, L.o_ids, L.verts, L.o_verts, p->c_cc[li],
+                                                          p->c_cs[li], (int)n, more ? p->c_cc[li + 1] : nullptr,
+                                                          more ? p->c_cs[li + 1] : nullptr,
+                                                          more ? p->c_ep[li] : nullptr);
     lc.after("k_crease_edges");
-    size_t tb = p->c_tmp_bytes;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(p->c_tmp, tb, p->c_kin, p->c_kout, p->c_vin, p->c_vout,
-                                                    (int)(2 * n), 0, 64, str);
-    if (e != cudaSuccess && !lc.err) {
-        lc.err = cuda_status(e);
-        g_detail = std::string("crease sort: ") + cudaGetErrorString(e);
-    }
-    lc.after("sort(creases)");
-    k_crease_verts<<<grid_for(2 * n), kBlock, 0, str>>>(p->c_kout, p->c_vout, (int)(2 * n), p->c_cs[li], p->c_bnd0,
-                                                        (int)L0.V, L.verts, L.o_verts);
+    CreaseEps eps{};
+    for (int t = 0; t < li; ++t) eps.epid[t] = p->c_ep[t];
+    const int64_t nv = (int64_t)V0 + m * ((1ll << li) - 1);
+    k_crease_verts<QUAD><<<grid_for(nv), kBlock, 0, str>>>(fc, li, V0, m, L.ids, p->c_cc[li], p->c_cs[li],
+                                                           p->c_vcnt, p->c_vptr, p->c_inc, p->c_bnd0, eps, L.verts,
+                                                           L.o_verts);
     lc.after("k_crease_verts");
+}
+
+void launch_creases(slak_plan* p, int li, Lc& lc)
+{
+    const Level& L = p->lv[li];
+    if (L.quad) launch_creases_t<true>(p, li, Faces<true>{nullptr, nullptr}, lc);
+    else launch_creases_t<false>(p, li, Faces<false>{L.ptr, p->s.cface}, lc);
 }
 
 int enqueue_all(slak_plan* p, cudaStream_t str)
@@ -677,22 +679,22 @@ void plan_carve(slak_plan* p, Carver& cv)
     }
     p->st = cv.take<DevStatus>(1);
     if (p->crease_levels > 0) {
-        const int64_t m = p->ncrease, nmax = m << (p->crease_levels - 1);
+        const int64_t m = p->ncrease;
         p->c_pairs = cv.take<int>(2 * m);
         p->c_sharp = cv.take<float>(m);
         p->c_mark = cv.take<int>(p->lv[0].N);
         p->c_bnd0 = p->lv[0].B > 0 ? cv.take<unsigned char>(p->lv[0].V) : nullptr;
+        p->c_vcnt = cv.take<int>(p->lv[0].V);
+        p->c_vptr = cv.take<int>(p->lv[0].V + 1);
+        p->c_inc = cv.take<int>(2 * m);
         p->c_cc.assign(p->crease_levels, nullptr);
         p->c_cs.assign(p->crease_levels, nullptr);
+        p->c_ep.assign(p->crease_levels, nullptr);
         for (int l = 0; l < p->crease_levels; ++l) {
             p->c_cc[l] = cv.take<int>(m << l);
             p->c_cs[l] = cv.take<float>(m << l);
+            if (l + 1 < p->crease_levels) p->c_ep[l] = cv.take<int>(m << l);
         }
-        p->c_kin = cv.take<unsigned long long>(2 * nmax);
-        p->c_kout = cv.take<unsigned long long>(2 * nmax);
-        p->c_vin = cv.take<int>(2 * nmax);
-        p->c_vout = cv.take<int>(2 * nmax);
-        p->c_tmp = cv.take<char>((int64_t)p->c_tmp_bytes);
     }
 }
 
@@ -929,8 +931,8 @@ int plan_autotune(slak_plan* p, cudaStream_t str)
 
 // Plan creation; with `ws`, the arena and the status word come from the
 // workspace (the plan does not own them).
-// Crease list sizing from a host copy of the sharpness (one sync): levels with
-// a live crease, and the sort's scratch.
+// Crease list sizing from a host copy of the sharpness (one sync): the levels
+// with a live crease.
 static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, cudaStream_t str)
 {
     std::vector<float> h((size_t)m);
@@ -945,15 +947,9 @@ static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, cudaSt
     const int nlev = (int)p->lv.size();
     int cl = smax > 0.0f ? (int)std::ceil((double)smax) : 0;
     p->ncrease = m;
-    p->crease_levels = std::min(cl, nlev);
+    p->crease_levels = std::min(std::min(cl, nlev), kMaxCreaseLevels);
     if (p->crease_levels == 0) return SLAK_OK;
-    if ((m << p->crease_levels) >= (1ll << 30)) return SLAK_ERR_UNSUPPORTED;
-    const int n2 = (int)(2 * (m << (p->crease_levels - 1)));
-    size_t tb = 0;
-    e = cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                        (int*)nullptr, (int*)nullptr, n2, 0, 64, str);
-    if (e != cudaSuccess) return cuda_status(e);
-    p->c_tmp_bytes = tb;
+    if ((m << p->crease_levels) >= (1ll << 30) || m >= (1ll << 29)) return SLAK_ERR_UNSUPPORTED;
     return SLAK_OK;
 }
 

@@ -17,8 +17,32 @@ from .mesh import QUAD, TRI, Mesh
 
 
 def read_obj(path: str) -> Mesh:
+    return _read(path, None)
+
+
+def read_obj_creased(path: str):
+    """(mesh, (pairs, sharpness)) with the file's "t crease" tags as an (m, 2)
+    int32 array of 0-based vertex ids and m float32 sharpness values."""
+    cr = _abi.SlakCreases()
+    mesh = _read(path, cr)
+    try:
+        m = int(cr.count)
+        if m == 0:
+            return mesh, (np.zeros((0, 2), np.int32), np.zeros(0, np.float32))
+        pairs = np.ctypeslib.as_array(cr.verts, shape=(2 * m,)).copy().reshape(m, 2)
+        sharp = np.ctypeslib.as_array(cr.sharpness, shape=(m,)).copy()
+        return mesh, (pairs, sharp)
+    finally:
+        _abi.lib().slak_obj_free_creases(ctypes.byref(cr))
+
+
+def _read(path, cr) -> Mesh:
     c = _abi.SlakMesh()
-    _abi.check(_abi.lib().slak_obj_read(os.fsencode(path), ctypes.byref(c)), f"slak_obj_read({path})")
+    if cr is None:
+        rc = _abi.lib().slak_obj_read(os.fsencode(path), ctypes.byref(c))
+    else:
+        rc = _abi.lib().slak_obj_read_creased(os.fsencode(path), ctypes.byref(c), ctypes.byref(cr))
+    _abi.check(rc, f"slak_obj_read({path})")
     try:
         F, N, V = int(c.nfaces), int(c.nnz), int(c.nverts)
         arr = lambda p, n, t: np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(t)), shape=(n,)).copy()
@@ -31,9 +55,10 @@ def read_obj(path: str) -> Mesh:
         _abi.lib().slak_obj_free(ctypes.byref(c))
 
 
-def write_obj(path: str, mesh) -> None:
+def write_obj(path: str, mesh, creases=None) -> None:
     """Writes a host mesh (a Mesh, or any object with its fields, e.g. a
-    refined HostResult); QUAD and TRI meshes need no face offsets."""
+    refined HostResult); QUAD and TRI meshes need no face offsets.  With
+    ``creases`` = (pairs, sharpness), one "t crease" tag per pair follows."""
     keep = []
 
     def p(a, dt):
@@ -49,4 +74,15 @@ def write_obj(path: str, mesh) -> None:
     c.ptr = p(None if mesh.type in (QUAD, TRI) else mesh.ptr, np.int32)
     c.ids = p(mesh.ids, np.int32)
     c.verts = p(np.asarray(mesh.verts, np.float32).reshape(-1), np.float32)
-    _abi.check(_abi.lib().slak_obj_write(os.fsencode(path), ctypes.byref(c)), f"slak_obj_write({path})")
+    if creases is None:
+        rc = _abi.lib().slak_obj_write(os.fsencode(path), ctypes.byref(c))
+    else:
+        pairs = np.ascontiguousarray(np.asarray(creases[0], np.int32).reshape(-1, 2))
+        sharp = np.ascontiguousarray(np.asarray(creases[1], np.float32).reshape(-1))
+        keep += [pairs, sharp]
+        cr = _abi.SlakCreases()
+        cr.count = sharp.size
+        cr.verts = pairs.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        cr.sharpness = sharp.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        rc = _abi.lib().slak_obj_write_creased(os.fsencode(path), ctypes.byref(c), ctypes.byref(cr))
+    _abi.check(rc, f"slak_obj_write({path})")

@@ -22,3 +22,27 @@ def test_obj_subdivide_round_trip(tmp_path, scheme):
     assert got.type == QUAD and got.nfaces == ref.nfaces and got.nverts == ref.nverts
     assert np.array_equal(got.ids, ref.ids)
     assert np.array_equal(got.verts[:, :3].view(np.uint32), ref.verts[:, :3].view(np.uint32))
+
+
+@pytest.mark.parametrize("scheme", ["slak", "lak"])
+def test_obj_crease_tags_subdivide(tmp_path, scheme):
+    """A file with "t crease" tags is refined with its creases: the result
+    reads back as the crease restatement's refined mesh."""
+    from oracle import creases as oc
+    src = meshgen.mixed_torus(24, 20, 0.05, 0.03, 0.005, seed=9)
+    ids = np.asarray(src.ids)
+    ptr = np.asarray(src.ptr)
+    first = ptr[:-1]
+    rng = np.random.default_rng(3)
+    pick = first[rng.random(first.size) < 0.2]
+    pairs = np.stack([ids[pick], ids[pick + 1]], 1).astype(np.int32)       # each face's first edge
+    pairs = np.unique(np.sort(pairs, 1), axis=0)
+    sharp = rng.choice(np.array([0.5, 1.0, 2.5, 4.0], np.float32), pairs.shape[0])
+    inp, out = tmp_path / "in.obj", tmp_path / "out.obj"
+    meshio.write_obj(str(inp), src, creases=(pairs, sharp))
+    assert objsubdiv.main([str(inp), str(out), "--levels", "3", "--scheme", scheme]) == 0
+    got = meshio.read_obj(str(out))
+    mesh, cr = meshio.read_obj_creased(str(inp))
+    ref = oc.subdivide_creased(mesh, 3, SLAK if scheme == "slak" else LAK, *cr)
+    assert np.array_equal(got.ids, ref.ids)
+    assert np.array_equal(got.verts[:, :3].view(np.uint32), ref.verts[:, :3].view(np.uint32))

@@ -103,3 +103,74 @@ def test_malformed_faces_rejected(tmp_path, bad):
 def test_missing_file_rejected(tmp_path):
     with pytest.raises(_abi.SlakError):
         meshio.read_obj(str(tmp_path / "none.obj"))
+
+
+CREASED = """v 0 0 0
+v 1 0 0
+v 1 1 0
+v 0 1 0
+v 0.5 0.5 1
+f 1 2 3 4
+t crease 2/1/0 0 1 4.5
+t crease 3/1/0 1 2 3 2
+t corner 1/1/0 4 10
+t crease 3/2/0 3 0 4 0.5 1.5
+t interpolateboundary 1/0/0 1
+"""
+
+
+def test_crease_tags(tmp_path):
+    path = tmp_path / "c.obj"
+    path.write_text(CREASED)
+    m, (pairs, sharp) = meshio.read_obj_creased(str(path))
+    assert m.nfaces == 1 and m.nverts == 5
+    assert pairs.tolist() == [[0, 1], [1, 2], [2, 3], [3, 0], [0, 4]]
+    assert sharp.tolist() == [4.5, 2.0, 2.0, 0.5, 1.5]
+    # the plain reader skips tags; a file without tags has no creases
+    assert np.array_equal(meshio.read_obj(str(path)).ids, m.ids)
+    plain = tmp_path / "p.obj"
+    plain.write_text(SAMPLE)
+    assert meshio.read_obj_creased(str(plain))[1][1].size == 0
+
+
+def test_crease_tags_round_trip(tmp_path):
+    m = meshgen.torus(12, 8, seed=2)
+    rng = np.random.default_rng(1)
+    ids = np.asarray(m.ids).reshape(-1, 4)
+    pairs = np.stack([ids[:, 0], ids[:, 1]], 1)[rng.random(ids.shape[0]) < 0.3].astype(np.int32)
+    sharp = rng.random(pairs.shape[0]).astype(np.float32) * 5
+    path = tmp_path / "t.obj"
+    meshio.write_obj(str(path), m, creases=(pairs, sharp))
+    r, (p2, s2) = meshio.read_obj_creased(str(path))
+    assert np.array_equal(r.ids, m.ids)
+    assert np.array_equal(p2, pairs) and np.array_equal(s2.view(np.uint32), sharp.view(np.uint32))
+
+
+def test_crease_tags_across_parallel_chunks(tmp_path):
+    rng = np.random.default_rng(9)
+    n = 150000
+    lines = [f"v {rng.normal():.6f} {rng.normal():.6f} {rng.normal():.6f}" for _ in range(n)]
+    expect = []
+    for k in range(0, n - 1, 37):
+        lines.insert(k + len(expect), f"t crease 2/1/0 {k} {k + 1} {k % 7 + 0.5}")
+        expect.append((k, k + 1, k % 7 + 0.5))
+    lines += ["f 1 2 3"]
+    path = tmp_path / "big.obj"
+    path.write_text("\n".join(lines) + "\n")
+    m, (pairs, sharp) = meshio.read_obj_creased(str(path))
+    assert m.nverts == n
+    assert pairs.tolist() == [[a, b] for a, b, _ in expect]
+    assert np.allclose(sharp, [s for _, _, s in expect])
+
+
+@pytest.mark.parametrize("bad", ["v 0 0 0\nv 1 0 0\nt crease 2/1/0 0 5 1\n",     # id out of range
+                                 "v 0 0 0\nv 1 0 0\nt crease 1/1/0 0 1\n",       # one id
+                                 "v 0 0 0\nv 1 0 0\nt crease 2/2/0 0 1 1 2\n",   # float count
+                                 "v 0 0 0\nv 1 0 0\nt crease 2/1/0 0 x 1\n",     # not a number
+                                 "v 0 0 0\nv 1 0 0\nt crease 2 1 0 0 1 1\n"])    # counts not n/n/n
+def test_malformed_crease_tags_rejected(tmp_path, bad):
+    path = tmp_path / "bad.obj"
+    path.write_text(bad)
+    with pytest.raises(_abi.SlakError):
+        meshio.read_obj_creased(str(path))
+    meshio.read_obj(str(path))           # the plain reader skips tags
