@@ -791,18 +791,6 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
 }
 
 // ---------------------------------------------------------------------------------------------
-// t of a general level feeding the fast path (SLAK): t[x] = slot[tw[prev x]],
-// -1 where prev(x) has no twin
-template <bool QUAD>
-__global__ void k_export_t(Faces<QUAD> fc, int N, const int* __restrict__ slot, const int* __restrict__ tw,
-                           int* __restrict__ t)
-{
-    int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= N) return;
-    const int tp = tw[fc.prev(x)];
-    t[x] = tp >= 0 ? slot[tp] : -1;
-}
-
 // 1 for each edge of a general level without a twin (H holds -1), the input of
 // the scan that gives the edges' boundary ranks to the first fast level
 __global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restrict__ isb)

@@ -3,8 +3,10 @@
 // One level turns a control mesh (F faces, N corners, V vertices) into an
 // all-quad mesh.  The general path rebuilds the vertex adjacency every level:
 //
-//   k_face_map   corner -> face (polygon levels)        createThreadFaceMapping, CatmullClarkKernels.cuh:189-198
-//   k_valence    corners per vertex                       evaluateValences, :137-145
+//   k_face_map_valence  corner -> face and corners per vertex (polygon levels)
+//                                                         createThreadFaceMapping, CatmullClarkKernels.cuh:189-198,
+//                                                         + evaluateValences, :137-145
+//   k_valence    corners per vertex (quad levels)         evaluateValences, :137-145
 //   scan         adjacency offsets                        cub_wrappers.cuh:30-43
 //   k_bucket     corners into their vertex's column       evaluateAdjacencies[Quad], :147-187
 //   k_vsort      column sorted by corner index, plus the vertex after / before
@@ -13,7 +15,7 @@
 //                (SLAK: checkForBoundary*, :200-321; LAK: the M^T M pattern of spgemm.cuh:61-100)
 //   scan         edge offsets                             CatmullClarkImpl.cu:209-211
 //   k_eids_*     edge id of every half-edge + edge -> half-edge table
-//   k_refine     refined quads                            refineTopology*, :405-575; LAKCatmullClarkKernels.cuh:320-431
+//   k_refine     refined quads (+ the fast path's t)      refineTopology*, :405-575; LAKCatmullClarkKernels.cuh:320-431
 //
 // The reference assigns adjacency slots with atomicAdd, so its edge numbering
 // changes from run to run.  Here every column is sorted by corner index, which
@@ -27,14 +29,22 @@ namespace slak {
 
 enum : int { SF_OWNER = 1, SF_BOUT = 2, SF_BIN = 4 };
 
-__global__ void k_face_map(const int* __restrict__ ptr, int F, int N, int* __restrict__ cface, DevStatus* st)
+// polygon levels: corner -> face (validating ptr) and the valences in one pass
+// over the faces
+__global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
+                                   int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f == 0 && (ptr[0] != 0 || ptr[F] != N)) set_error(st, 4, -1);
     if (f >= F) return;
     int b = ptr[f], e = ptr[f + 1];
     if (b < 0 || e > N || e - b < 3) { set_error(st, 4, f); return; }
-    for (int c = b; c < e; ++c) cface[c] = f;
+    for (int c = b; c < e; ++c) {
+        cface[c] = f;
+        const int v = __ldg(ids + c);
+        if ((unsigned)v >= (unsigned)V) { set_error(st, 4, c); continue; }
+        atomicAdd(cnt + v, 1);
+    }
 }
 
 __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
@@ -251,12 +261,21 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
 }
 
 // SLAK edge ids: owners in slot order get eptr[v] + rank; the twin shares it.
+// Thread 0 of k_eids_* also checks the level's edge and boundary counts
+// against the sizes the plan was made for (a topology change since creation).
+__device__ __forceinline__ void check_level(int v, const int* eptr, int V, int E, const int* bcount, int B,
+                                            DevStatus* st, int li)
+{
+    if (v == 0 && (eptr[V] != E || *bcount != B)) set_error(st, 4, 1000 + li);
+}
+
 __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
                             const int* __restrict__ stw, const int* __restrict__ sflag,
                             const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
-                            int2* __restrict__ H, DevStatus* st)
+                            int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
 {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
+    check_level(v, eptr, V, Ecap, bcount, B, st, li);
     if (v >= V) return;
     int id = eptr[v];
     for (int s = sptr[v]; s < sptr[v + 1]; ++s) {
@@ -274,9 +293,11 @@ __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __re
 __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
                            const int* __restrict__ snext, const int* __restrict__ sprev,
                            const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
-                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st)
+                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
+                           int li)
 {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
+    check_level(v, eptr, V, Ecap, bcount, B, st, li);
     if (v >= V) return;
     const int b = sptr[v], e = sptr[v + 1];
     int id = eptr[v], last = -1;
@@ -313,16 +334,24 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
 }
 
 // refined quad of corner c: {v, V+F+e_out, V+face, V+F+e_in}
+// With `xt` (a SLAK level whose state feeds the fast path) it also exports
+// t[c] = slot[twin(prev c)], -1 where prev(c) has no twin.
 template <bool QUAD, bool LAK>
 __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
                          int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
-                         int4* __restrict__ out_vals)
+                         int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
+                         int* __restrict__ xt)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     const int VF = V + F;
-    int4 q = make_int4(__ldg(ids + c), VF + __ldg(eid + c), V + fc.face(c), VF + __ldg(eid + fc.prev(c)));
+    const int p = fc.prev(c);
+    int4 q = make_int4(__ldg(ids + c), VF + __ldg(eid + c), V + fc.face(c), VF + __ldg(eid + p));
     __stcs(out_ids + c, q);
+    if (xt) {
+        const int tp = __ldg(xtw + p);
+        xt[c] = tp >= 0 ? __ldg(xslot + tp) : -1;
+    }
     if (LAK && out_vals != nullptr) {          // only the final level stores ptr / vals
         __stcs(out_vals + c, make_int4(1, 2, 3, 4));
         out_ptr[c] = 4 * c;

@@ -3,7 +3,8 @@
 // Replaces CubFunctions::scan_exclusive (LibInclude/device/cub_wrappers.cuh:30-43):
 // out[0] = 0, out[i+1] = in[0] + ... + in[i], out has n+1 entries, so out[n] is
 // the total.  Reduce-then-scan over tiles of 2048 items: tile sums, one block
-// scanning the tile sums, then a tile scan with the tile's carry.  Integer and
+// scanning the tile sums, then a tile scan with the tile's carry (up to 2048
+// tiles, each tile's block sums the tile sums before it instead).  Integer and
 // deterministic.
 #pragma once
 
@@ -107,6 +108,54 @@ __global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ i
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tsum[nt];
 }
 
+// Up to kScanSmallTiles tiles: no separate scan of the tile sums; each block
+// adds up the sums of the tiles before it (and all of them, for out[n]).
+constexpr int kScanSmallTiles = 2048;
+
+__global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restrict__ in, int64_t n,
+                                                             const int* __restrict__ tsum, int nt,
+                                                             int* __restrict__ out)
+{
+    __shared__ int tile[kScanTile];
+    __shared__ int tot;
+    int before = 0, all = 0;
+    for (int k = threadIdx.x; k < nt; k += kBlock) {
+        const int x = tsum[k];
+        all += x;
+        if (k < (int)blockIdx.x) before += x;
+    }
+    block_excl_scan(before, &tot);
+    __syncthreads();
+    const int carry = tot;
+    __syncthreads();
+    block_excl_scan(all, &tot);
+    __syncthreads();
+    const int total = tot;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int j = i * kBlock + threadIdx.x;
+        int64_t k = base + j;
+        tile[j] = k < n ? in[k] : 0;
+    }
+    __syncthreads();
+    int loc[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) { loc[i] = s; s += tile[threadIdx.x * kScanItems + i]; }
+    int e = block_excl_scan(s, &tot) + carry;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) tile[threadIdx.x * kScanItems + i] = e + loc[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        int j = i * kBlock + threadIdx.x;
+        int64_t k = base + j;
+        if (k < n) out[k] = tile[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = total;
+}
+
 inline int64_t scan_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 // tmp must hold scan_tiles(n) + 1 ints
@@ -115,6 +164,11 @@ inline void scan_exclusive(const int* in, int* out, int64_t n, int* tmp, cudaStr
     int64_t nt = scan_tiles(n);
     if (nt < 1) nt = 1;
     k_scan_reduce<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp);
+    if (nt <= kScanSmallTiles) {
+        k_scan_final_small<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp, (int)nt, out);
+        if (launches) *launches += 2;
+        return;
+    }
     k_scan_tiles<<<1, kBlock, 0, s>>>(tmp, (int)nt);
     k_scan_final<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp, (int)nt, out);
     if (launches) *launches += 3;

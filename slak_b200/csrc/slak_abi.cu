@@ -234,14 +234,15 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
 {
     const int F = (int)L.F, V = (int)L.V, N = (int)L.N;
     cudaStream_t str = lc.s;
+    cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
     if (!L.quad) {
         cudaMemsetAsync(s.cface, 0, sizeof(int) * (size_t)N, str);
-        k_face_map<<<grid_for(F), kBlock, 0, str>>>(L.ptr, F, N, s.cface, st);
-        lc.after("k_face_map");
+        k_face_map_valence<<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, F, N, V, s.cface, s.cnt, st);
+        lc.after("k_face_map_valence");
+    } else {
+        k_valence<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.cnt, st);
+        lc.after("k_valence");
     }
-    cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
-    k_valence<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.cnt, st);
-    lc.after("k_valence");
     int64_t dummy = 0;
     scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, &dummy);
     lc.after("scan(valence)", 3);
@@ -282,31 +283,33 @@ __global__ void k_quad_ptr_vals(int N, int* __restrict__ ptr, int4* __restrict__
     if (c == N - 1) ptr[N] = 4 * N;
 }
 
-__global__ void k_check_level(const int* eptr, int V, const int* bcount, int E, int B, DevStatus* st, int li)
-{
-    if (eptr[V] != E || *bcount != B) set_error(st, 4, 1000 + li);
-}
-
+// The rest of a general level, after launch_topology_a: edge ids (with the
+// check of the level's counts), refined quads (and, for a SLAK level feeding
+// the fast path, t), face, edge and vertex points.
 template <bool QUAD>
-void launch_rest(const Level& L, int scheme, bool compensated, Scratch& s, DevStatus* st, Lc& lc)
+void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& s, DevStatus* st, Lc& lc)
 {
     const int F = (int)L.F, V = (int)L.V, N = (int)L.N, E = (int)L.E;
     const bool lak = scheme == SLAK_SCHEME_LAK;
     cudaStream_t str = lc.s;
     Faces<QUAD> fc{L.ptr, s.cface};
+    const int* bcount = &st->bcount[li];
     if (lak)
         k_eids_lak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
-                                                     s.H, st);
+                                                     s.H, st, bcount, (int)L.B, li);
     else
-        k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st);
+        k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
+                                                      bcount, (int)L.B, li);
     lc.after("k_eids");
     if (lak)
         k_refine<QUAD, true><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
                                                               reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
-                                                              reinterpret_cast<int4*>(L.o_vals));
+                                                              reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
+                                                              nullptr);
     else
         k_refine<QUAD, false><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
-                                                               reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr);
+                                                               reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
+                                                               s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
     lc.after("k_refine");
     float* R = L.o_verts;
     float* FPo = R + 4 * (size_t)V;
@@ -476,20 +479,9 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
             continue;
         }
         launch_topology_a(L, (int)li, p->scheme, p->s, p->st, lc);
-        k_check_level<<<1, 1, 0, str>>>(p->s.eptr, (int)L.V, &p->st->bcount[li], (int)L.E, (int)L.B, p->st,
-                                         (int)li);
-        lc.after("k_check_level");
-        if (L.quad) launch_rest<true>(L, p->scheme, comp, p->s, p->st, lc);
-        else launch_rest<false>(L, p->scheme, comp, p->s, p->st, lc);
-        if (L.export_state && p->scheme == SLAK_SCHEME_SLAK) {   // slot / twin came from k_vsort / k_edges
-            if (L.quad)
-                k_export_t<true><<<grid_for(L.N), kBlock, 0, str>>>(Faces<true>{L.ptr, p->s.cface}, (int)L.N,
-                                                                    p->s.xslot, p->s.xtw, p->s.xt);
-            else
-                k_export_t<false><<<grid_for(L.N), kBlock, 0, str>>>(Faces<false>{L.ptr, p->s.cface}, (int)L.N,
-                                                                     p->s.xslot, p->s.xtw, p->s.xt);
-            lc.after("k_export_t");
-        }
+        // slot / twin of an exported SLAK state come from k_vsort / k_edges, t from k_refine
+        if (L.quad) launch_rest<true>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
+        else launch_rest<false>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
         if (L.export_state && L.B > 0) {     // the edges' boundary ranks
             k_export_bflag<<<grid_for(L.E), kBlock, 0, str>>>((int)L.E, p->s.H, p->s.xisb);
             lc.after("k_export_bflag");
@@ -1659,8 +1651,8 @@ extern "C" int slak_subdivide_level_noalloc(const slak_mesh* cm, slak_mesh* rm, 
     L.o_ids = rm->ids; L.o_verts = rm->verts;
     L.o_ptr = lak ? rm->ptr : nullptr;
     L.o_vals = lak ? rm->vals : nullptr;
-    if (quad) launch_rest<true>(L, scheme, false, s, st, lc);
-    else launch_rest<false>(L, scheme, false, s, st, lc);
+    if (quad) launch_rest<true>(L, 0, scheme, false, s, st, lc);
+    else launch_rest<false>(L, 0, scheme, false, s, st, lc);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
     cudaMemcpyAsync(&h, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
