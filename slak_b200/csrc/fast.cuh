@@ -495,17 +495,16 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
             for (int j = 0; j < 8; ++j)
                 if (j < k) yv = f4_add(yv, f4_div(fq[j], nn));
             const int64_t VFc = (int64_t)d.V + d.N1;
-            float4 fprev = fq[0];
-#pragma unroll
-            for (int j = 1; j < 8; ++j)
-                if (j == k - 1) fprev = fq[j];
+            // FP of the last corner (the first corner's prev) loaded again, an L1
+            // hit: selecting fq[k-1] would index the array dynamically and put it
+            // in local memory
+            const float4 flast = ldg4(FP, e - 1);
 #pragma unroll
             for (int j = 0; j < 8; ++j)
                 if (j < k) {
                     const float4 ta = f4_mul(f4_add(c2, fq[j]), 0.25f);
-                    const float4 tb = f4_mul(f4_add(pe[j], fprev), 0.25f);
+                    const float4 tb = f4_mul(f4_add(pe[j], j == 0 ? flast : fq[j > 0 ? j - 1 : 0]), 0.25f);
                     st4_cs(R, VFc + d.N1 + b + j, f4_add(f4_add(f4_zero(), ta), tb));
-                    fprev = fq[j];
                 }
         } else {
 #pragma unroll
