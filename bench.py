@@ -387,7 +387,9 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws, creases=None):
             times.append(dt)
     t = _max_over_ranks(dist, statistics.mean(times))
     return {"value": faces * ws / t, "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3}
+            "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3,
+            "ms_spread": {"min": min(times) * 1e3, "median": statistics.median(times) * 1e3,
+                          "max": max(times) * 1e3, "steps": len(times)}}
 
 
 def batch_shard(count, rank=0, ws=1):
@@ -610,7 +612,9 @@ def run_reference(args, dist, rank, ws):
                          "sample": "GPUPeople/SLAK's own CUDA path (built for sm_100a) on the full workload; "
                                    "the reference has no CPU implementation"},
         "e2e": {"value": faces / (e2e_t * 1e-3), "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t},
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t,
+                "ms_spread": {"min": min(e2e_ms), "median": statistics.median(e2e_ms), "max": max(e2e_ms),
+                              "steps": len(e2e_ms)}},
         "clocks": clk.summary(),
     }
 
