@@ -304,6 +304,18 @@ int slak_batch_num_waves(const slak_batch* batch);
 int64_t slak_batch_launches(const slak_batch* batch);
 int slak_batch_destroy(slak_batch* batch);
 
+/*
+ * The batch in one call: rmeshes[i] receives meshes[i] refined to levels[i].
+ * This is the batched counterpart of slak_subdivide, and of the reference's
+ * per-mesh loop (source/main.cpp:84-113). Each output array has its own
+ * cudaMalloc and belongs to the caller, who frees it with slak_mesh_free or
+ * cudaFree, as after slak_subdivide. A mesh with nothing to refine leaves
+ * rmeshes[i] zeroed. The call returns once every mesh is refined. All
+ * outputs are resident at once; the scratch runs in waves.
+ */
+int slak_subdivide_batched(const slak_mesh* meshes, const int* levels, int64_t count, int scheme,
+                           slak_mesh* rmeshes, slak_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

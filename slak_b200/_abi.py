@@ -26,7 +26,7 @@ EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
-           "slak_plan_destroy", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
+           "slak_plan_destroy", "slak_subdivide_batched", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
            "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
 
 
@@ -119,6 +119,8 @@ def lib():
         L.slak_autotune_reset.argtypes = []
         L.slak_autotune_reset.restype = I
         L.slak_batch_create.argtypes = [P, ctypes.POINTER(ctypes.c_int), I64, I, I, V, ctypes.POINTER(V)]
+        L.slak_subdivide_batched.argtypes = [P, ctypes.POINTER(ctypes.c_int), I64, I, P, V]
+        L.slak_subdivide_batched.restype = I
         L.slak_batch_execute.argtypes = [V, V]
         L.slak_batch_status.argtypes = [V, V]
         L.slak_batch_output.argtypes = [V, I64, P]

@@ -265,6 +265,24 @@ def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0, creas
     return out
 
 
+def subdivide_batched(meshes: List[DeviceMesh], levels: List[int], scheme: int, stream=None) -> List[DeviceMesh]:
+    """slak_subdivide_batched: every mesh refined in one call; each result owns
+    its device arrays (freed with the returned DeviceMesh)."""
+    n = len(meshes)
+    arr = (_abi.SlakMesh * max(n, 1))()
+    for i, m in enumerate(meshes):
+        arr[i] = m.as_c()
+    lv = (ctypes.c_int * max(n, 1))(*[int(l) for l in levels])
+    out = (_abi.SlakMesh * max(n, 1))()
+    rc = _abi.lib().slak_subdivide_batched(arr, lv, n, int(scheme), out, _stream_handle(stream))
+    _abi.check(rc, "slak_subdivide_batched")
+    res = []
+    for i in range(n):
+        c = out[i]
+        res.append(_wrap_c(c, _OwnedMesh(c)) if c.nfaces else DeviceMesh())
+    return res
+
+
 class Batch:
     """Many meshes, each with its own level count, in one call (slak_batch_*).
 

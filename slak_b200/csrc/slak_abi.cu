@@ -1265,6 +1265,8 @@ struct slak_batch {
     DevStatus* d_st = nullptr;                  // device, one per mesh (outlives the waves' arenas)
     int64_t launches = 0;
     int executed = 0;
+    bool per_mesh_out = false;                  // outputs allocated per mesh (slak_subdivide_batched)
+    std::vector<char> out_given;                // per mesh: arrays handed to the caller
 };
 
 namespace {
@@ -1280,6 +1282,15 @@ void batch_free(slak_batch* b)
     for (auto e : b->fork) cudaEventDestroy(e);
     for (auto e : b->join) cudaEventDestroy(e);
     if (b->out_mem) cudaFree(b->out_mem);
+    if (b->per_mesh_out)
+        for (size_t i = 0; i < b->outs.size(); ++i)
+            if (!b->out_given[i]) {
+                slak_mesh& m = b->outs[i];
+                if (m.ids) cudaFree(m.ids);
+                if (m.verts) cudaFree(m.verts);
+                if (m.ptr) cudaFree(m.ptr);
+                if (m.vals) cudaFree(m.vals);
+            }
     if (b->arena) cudaFree(b->arena);
     if (b->d_st) cudaFree(b->d_st);
     if (b->h_st) cudaFreeHost(b->h_st);
@@ -1320,8 +1331,12 @@ int batch_enqueue(slak_batch* b, cudaStream_t str)
 
 extern "C" {
 
-int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
-                      slak_stream_t stream, slak_batch** out_batch)
+}  // extern "C"
+
+// per_mesh_out: every mesh's output arrays come from their own cudaMalloc, so
+// they can be handed to the caller (slak_subdivide_batched)
+static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
+                             slak_stream_t stream, slak_batch** out_batch, bool per_mesh_out)
 {
     if (!meshes || !levels || count < 0 || !out_batch) return SLAK_ERR_INVALID_ARG;
     *out_batch = nullptr;
@@ -1329,8 +1344,10 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
     if (!b) return SLAK_ERR_OOM;
     b->scheme = scheme;
     b->flags = flags;
+    b->per_mesh_out = per_mesh_out;
     b->plans.assign(count, nullptr);
     b->outs.assign(count, slak_mesh{});
+    b->out_given.assign(count, 0);
     cudaStream_t str = reinterpret_cast<cudaStream_t>(stream);
     int rc = SLAK_OK;
     int64_t maxN = 0, maxV = 0;
@@ -1441,14 +1458,27 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
         if (!cur.empty()) { b->waves.push_back(cur); b->arena_bytes = std::max(b->arena_bytes, cur_b); }
     }
     if (rc == SLAK_OK && total_out) {
-        ce = cudaMalloc(&b->out_mem, total_out);
+        if (!b->per_mesh_out) ce = cudaMalloc(&b->out_mem, total_out);
         if (ce == cudaSuccess && b->arena_bytes) ce = cudaMalloc(&b->arena, b->arena_bytes);
         if (ce == cudaSuccess) ce = cudaMalloc(&b->d_st, sizeof(DevStatus) * (size_t)count);
         if (ce != cudaSuccess) rc = cuda_status(ce);
     }
+    if (rc == SLAK_OK && b->per_mesh_out) {
+        for (int64_t i = 0; i < count && ce == cudaSuccess; ++i) {
+            if (!b->plans[i]) continue;
+            slak_mesh& m = b->outs[i];
+            ce = cudaMalloc(&m.ids, sizeof(int) * (size_t)m.nnz);
+            if (ce == cudaSuccess) ce = cudaMalloc(&m.verts, sizeof(float) * 4 * (size_t)m.nverts);
+            if (ce == cudaSuccess && scheme == SLAK_SCHEME_LAK) {
+                ce = cudaMalloc(&m.ptr, sizeof(int) * (size_t)(m.nfaces + 1));
+                if (ce == cudaSuccess) ce = cudaMalloc(&m.vals, sizeof(int) * (size_t)m.nnz);
+            }
+        }
+        if (ce != cudaSuccess) rc = cuda_status(ce);
+    }
     if (rc == SLAK_OK) {
         char* o = static_cast<char*>(b->out_mem);
-        for (int64_t i = 0; i < count; ++i) {
+        for (int64_t i = 0; i < count && !b->per_mesh_out; ++i) {
             if (!b->plans[i]) continue;
             slak_mesh& m = b->outs[i];
             m.ids = reinterpret_cast<int*>(o); o += align_up(sizeof(int) * (size_t)m.nnz);
@@ -1491,6 +1521,34 @@ int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count,
     if (rc != SLAK_OK) { batch_free(b); return rc; }
     *out_batch = b;
     return SLAK_OK;
+}
+
+extern "C" {
+
+int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
+                      slak_stream_t stream, slak_batch** out_batch)
+{
+    return batch_create_impl(meshes, levels, count, scheme, flags, stream, out_batch, false);
+}
+
+int slak_subdivide_batched(const slak_mesh* meshes, const int* levels, int64_t count, int scheme,
+                           slak_mesh* rmeshes, slak_stream_t stream)
+{
+    if (!rmeshes || count < 0) return SLAK_ERR_INVALID_ARG;
+    for (int64_t i = 0; i < count; ++i) std::memset(&rmeshes[i], 0, sizeof(slak_mesh));
+    slak_batch* b = nullptr;
+    int rc = batch_create_impl(meshes, levels, count, scheme, 0, stream, &b, true);   // one execution: eager
+    if (rc != SLAK_OK) return rc;
+    rc = slak_batch_execute(b, stream);
+    if (rc == SLAK_OK) rc = slak_batch_status(b, stream);
+    if (rc == SLAK_OK)
+        for (int64_t i = 0; i < count; ++i) {
+            if (!b->plans[i]) continue;
+            rmeshes[i] = b->outs[i];
+            b->out_given[i] = 1;
+        }
+    batch_free(b);
+    return rc;
 }
 
 int slak_batch_execute(slak_batch* b, slak_stream_t stream)

@@ -60,3 +60,32 @@ def test_batch_matches_single(scheme, mode, monkeypatch):
             assert np.array_equal(h.ptr, ref.ptr) and np.array_equal(h.vals, ref.vals)
     assert b.launches > 0
     b.close()
+
+
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+@pytest.mark.parametrize("waves", [False, True])
+def test_subdivide_batched_one_call(scheme, waves, monkeypatch):
+    """slak_subdivide_batched: caller-owned outputs, each equal to
+    slak_subdivide on that mesh alone; meshes with nothing to refine stay zeroed."""
+    import torch
+    items = _meshes()
+    if scheme == LAK:
+        items = [(m if m.ptr is not None else m.with_quad_ptr(), l) for m, l in items]
+    if waves:
+        monkeypatch.setenv("SLAK_BATCH_WAVE_BYTES", str(8 << 20))
+    dms = [api.DeviceMesh.from_host(m) for m, _ in items]
+    outs = api.subdivide_batched(dms, [l for _, l in items], scheme)
+    torch.cuda.synchronize()
+    for (m, l), o in zip(items, outs):
+        if m.type == QUAD and l <= 0:
+            assert o.nfaces == 0 and o.ids is None
+            continue
+        h = o.to_host()
+        ref = api.subdivide(m, l, scheme)
+        assert (h.nfaces, h.nverts, h.nnz) == (ref.nfaces, ref.nverts, ref.nnz)
+        assert np.array_equal(h.ids, ref.ids)
+        assert np.array_equal(_bits(h.verts), _bits(ref.verts))
+        if scheme == LAK:
+            assert np.array_equal(h.ptr, ref.ptr) and np.array_equal(h.vals, ref.vals)
+    del outs                                   # the caller's arrays go back through slak_mesh_free
+    torch.cuda.synchronize()
