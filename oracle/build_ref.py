@@ -1,4 +1,5 @@
-"""Recipe: compile GPUPeople/SLAK's own CUDA sources for sm_100a.
+"""Recipe: compile GPUPeople/SLAK's own CUDA sources for sm_100a, and its
+driver program against this repository's drop-in headers.
 
 TEST / BASELINE INFRASTRUCTURE ONLY.  The reference's files are compiled
 where they lie (never copied); outputs go to oracle/_ref/ only.  The
@@ -54,6 +55,41 @@ def build(ref_root: str, out_dir: str, nvcc: str = "nvcc", verbose: bool = False
     return target
 
 
+def build_dropin_main(ref_root: str, out_dir: str, include_dir: str, lib_dir: str, cuda_home: str = "/usr/local/cuda",
+                      cxx: str = "g++", verbose: bool = False, force: bool = False):
+    """The reference's own driver (source/main.cpp), compiled unchanged against
+    this repository's drop-in headers (include/CatmullClark.h,
+    include/LAKCatmullClark.h, found first on the include path) and linked
+    with libslak_b200.so instead of the reference's library.  Its mesh I/O
+    headers (include/Mesh.h, include/obj.h, LibInclude/cuda_host_helpers.h,
+    LibInclude/math/) are the reference's, read where they lie."""
+    src = os.path.join(ref_root, "source", "main.cpp")
+    lib = os.path.join(lib_dir, "libslak_b200.so")
+    for f in (src, lib):
+        if not os.path.exists(f):
+            raise FileNotFoundError(f)
+    os.makedirs(out_dir, exist_ok=True)
+    target = os.path.join(out_dir, "slak_main_dropin")
+    deps = [src, lib, os.path.join(include_dir, "CatmullClark.h"), os.path.join(include_dir, "LAKCatmullClark.h")]
+    if not force and os.path.exists(target) and all(os.path.getmtime(d) <= os.path.getmtime(target) for d in deps):
+        return target
+    rel = os.path.relpath(lib_dir, out_dir)
+    cmd = [cxx, "-std=c++17", "-O2", "-w", "-I", include_dir, "-I", os.path.join(ref_root, "include"),
+           "-I", os.path.join(ref_root, "LibInclude"), "-I", os.path.join(cuda_home, "include"), src,
+           "-L", lib_dir, "-lslak_b200", "-L", os.path.join(cuda_home, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN/" + rel, "-Wl,-rpath," + os.path.join(cuda_home, "lib64"), "-o", target]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("compiling the reference's main.cpp against the drop-in headers failed")
+    return target
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     print(build(root, os.path.join(HERE, "_ref"), verbose=True, force=True))
+    repo = os.path.dirname(HERE)
+    print(build_dropin_main(root, os.path.join(HERE, "_ref"), os.path.join(repo, "include"),
+                            os.path.join(repo, "slak_b200", "lib"), verbose=True, force=True))

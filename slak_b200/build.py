@@ -95,7 +95,8 @@ def build_oracle(verbose=False, force=False):
 
 
 def build_reference(verbose=False, force=False, ref_root="/root/reference"):
-    """Compiles the reference's CUDA sources (never copied) with oracle/build_ref.py."""
+    """Compiles the reference's CUDA sources (never copied) with oracle/build_ref.py,
+    and the reference's driver against the drop-in headers (oracle/_ref/slak_main_dropin)."""
     if not os.path.isdir(ref_root):
         return None
     sys.path.insert(0, _paths.REPO_DIR)
@@ -103,7 +104,10 @@ def build_reference(verbose=False, force=False, ref_root="/root/reference"):
         from oracle import build_ref
     finally:
         sys.path.pop(0)
-    return build_ref.build(ref_root, os.path.dirname(_paths.LIB_REF), nvcc=NVCC, verbose=verbose, force=force)
+    out = build_ref.build(ref_root, os.path.dirname(_paths.LIB_REF), nvcc=NVCC, verbose=verbose, force=force)
+    build_ref.build_dropin_main(ref_root, os.path.dirname(_paths.LIB_REF), _paths.INCLUDE_DIR, _paths.LIB_DIR,
+                                verbose=verbose, force=force)
+    return out
 
 
 def build_all(verbose=False, force=False):
