@@ -224,10 +224,14 @@ __device__ __forceinline__ void boundary_edge(const FastDims& d, QState& c, floa
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
 // BND: P has a boundary; tw / t of P are -1 where there is no twin, and P's
 // edges carry their boundary ranks.
+// optr / ovals (LAK, last level): the refined mesh's ptr[q] = 4q and
+// vals[q] = {1, 2, 3, 4}; they depend on q alone, so a block writes the 4 BS
+// refined quads of its span with consecutive threads (coalesced).
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
-                                           int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z)
+                                           int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
+                                           int* __restrict__ optr, int4* __restrict__ ovals)
 {
     // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores (consecutive
     // t) and the run-order reads (4 k's of a t, then the next t) are both free
@@ -422,6 +426,18 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
             edge_point_vertex<LAK, STATE, BND>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, fh2, c0, Pu, c1, c2, Pf2, fp,
                                                Fnh, Fh2, Fnh2, br_x);
         }
+    }
+    if (LAK && !STATE && optr != nullptr) {
+        const int64_t q0 = 4 * (int64_t)x0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t qq = q0 + threadIdx.x + (int64_t)j * BS;
+            if (qq < d.N) {
+                __stcs(ovals + qq, make_int4(1, 2, 3, 4));
+                __stcs(optr + qq, (int)(4 * qq));
+            }
+        }
+        if (x == 0) optr[d.N] = 4 * d.N;
     }
 }
 

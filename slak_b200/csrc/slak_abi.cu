@@ -274,14 +274,6 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     lc.after("scan(edges)", 3);
 }
 
-__global__ void k_quad_ptr_vals(int N, int* __restrict__ ptr, int4* __restrict__ vals)
-{
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= N) return;
-    __stcs(vals + c, make_int4(1, 2, 3, 4));
-    ptr[c] = 4 * c;
-    if (c == N - 1) ptr[N] = 4 * N;
-}
 
 // The rest of a general level, after launch_topology_a: edge ids (with the
 // check of the level's counts), refined quads (and, for a SLAK level feeding
@@ -347,13 +339,16 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     // must read once, and the refined ids / positions it alone writes
     const int64_t g1b = 4 * L.N + 16 * L.V + 16 * L.N + 16 * L.F + 16 * Pl.F + (LAK ? 0 : 16 * L.F);
     const int64_t g2b = 16 * Pl.E + (LAK ? 16 * 2 * L.F : 0);
+    // LAK's last level: the refined ptr / vals come from k_g1 too
+    int* optr = LAK && !STATE ? L.o_ptr : nullptr;
+    int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
         k_g1<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
                                                                          L.out_state, reinterpret_cast<int4*>(L.o_ids),
-                                                                         L.o_verts, L.slots);
+                                                                         L.o_verts, L.slots, optr, ovals);
     });
-    lc.after("k_g1", 1, PQ ? g1b + g2b : g1b);
+    lc.after("k_g1", 1, (PQ ? g1b + g2b : g1b) + (optr ? 4 * (L.N + 1) + 16 * L.N : 0));
     if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
         k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts,
                                                               comp ? 1 : 0);
@@ -398,10 +393,6 @@ void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, 
     else if (Pl.quad) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.B > 0) launch_fast_p<false, true>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     else launch_fast_p<false, false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
-    if (L.o_ptr) {   // LAK final level: quad offsets and corner positions
-        k_quad_ptr_vals<<<grid_for(L.N), kBlock, 0, lc.s>>>((int)L.N, L.o_ptr, reinterpret_cast<int4*>(L.o_vals));
-        lc.after("k_quad_ptr_vals");
-    }
 }
 
 // The crease pass of level li (after the level's own kernels): level 0 first
