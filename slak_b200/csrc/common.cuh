@@ -128,6 +128,44 @@ __device__ __forceinline__ void for_each_loaded(int n, Load load, Add add)
 // n selection passes that each wait for the previous minimum; for columns of
 // up to kRankMax slots (high-valence vertices; shorter ones stay in registers).
 constexpr int kRankMax = 64;
+
+// Columns longer than kBigCol slots (and up to kWarpCol) are taken by their
+// whole warp: loads and ranks in parallel into shared memory, then one lane
+// adds the sums in the fixed order (same bits as the single-thread paths).
+constexpr int kBigCol = 16;
+constexpr int kWarpCol = 64;
+
+__device__ __forceinline__ float4 shfl4(float4 v, int src)
+{
+    return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                       __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
+}
+
+// A long column's slots in its warp: slot k is element k >> 5 of lane k & 31
+// (two per lane for up to kWarpCol = 64 slots).  col4 / col1 fetch slot k
+// (k the same on every lane) from its lane; rank_of gives each of a lane's
+// keys its rank in ascending key order, ties by slot.
+__device__ __forceinline__ float4 col4(float4 e0, float4 e1, int k) { return shfl4(k < 32 ? e0 : e1, k & 31); }
+__device__ __forceinline__ int col1(int e0, int e1, int k) { return __shfl_sync(0xffffffffu, k < 32 ? e0 : e1, k & 31); }
+__device__ __forceinline__ void rank_of(int n, int key0, int key1, int& r0, int& r1)
+{
+    const int lane = threadIdx.x & 31;
+    r0 = 0;
+    r1 = 0;
+    for (int j = 0; j < n; ++j) {
+        const int y = col1(key0, key1, j);
+        r0 += (y < key0) | ((y == key0) & (j < lane));
+        r1 += (y < key1) | ((y == key1) & (j < lane + 32));
+    }
+}
+// The slot of rank r (r the same on every lane), as (lane, element).
+__device__ __forceinline__ void slot_of_rank(int r, bool h0, bool h1, int r0, int r1, int& src, int& el)
+{
+    const unsigned m0 = __ballot_sync(0xffffffffu, h0 && r0 == r);
+    const unsigned m1 = __ballot_sync(0xffffffffu, h1 && r1 == r);
+    el = m0 ? 0 : 1;
+    src = __ffs(m0 ? m0 : m1) - 1;
+}
 __device__ __forceinline__ void rank_order(const int* __restrict__ key, int b, int n, int* perm)
 {
     for (int k = 0; k < n; ++k) {

@@ -59,11 +59,6 @@ struct FastDims {
     int B1;                // P's boundary edges (0: closed)
 };
 
-__device__ __forceinline__ float4 shfl4(float4 v, int src)
-{
-    return make_float4(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
-                       __shfl_sync(0xffffffffu, v.z, src), __shfl_sync(0xffffffffu, v.w, src));
-}
 __device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
 {
     return make_float4(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
@@ -668,20 +663,13 @@ __device__ __forceinline__ float4 boundary_vertex(const float* __restrict__ P, c
 }
 
 // ---------------------------------------------------------------------------------------------
-// G3: one thread per vertex v of P.  Its column's records (written by k_g1 at
-// the column's slots) are contiguous, so the vertex point and, for SLAK, the
-// edge points of C's edges {v, e_out(x)} (ids = the slots) stream.  With a
-// boundary (BND), an edge {v, e_out(x)} without a twin gets the midpoint.
-template <bool LAK, bool STATE, int BS, bool BND = false>
-__global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
-                                           SlotScratch z, float* __restrict__ R, int compensated)
+// One vertex of P on its own thread (columns of up to kBigCol slots, and
+// columns too long for the warp path).
+template <bool LAK, bool STATE, bool BND>
+__device__ __forceinline__ void g3_vertex(FastDims d, const float* __restrict__ P, QState c, SlotScratch z,
+                                          float* __restrict__ R, int compensated, int v, int b, int n)
 {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= d.V1) {
-        if (STATE && v == d.V1) c.sptr[d.V] = d.N;
-        return;
-    }
-    const int b = __ldg(p.sptr + v), e = __ldg(p.sptr + v + 1), n = e - b;
+    const int e = b + n;
     const float4 Pv = ldg4(P, v);
     const float nn = (float)(n * n);
     const float4* Z = z.Z;
@@ -778,8 +766,8 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         // face points in column order, then the tails e_in(x) in ascending id
         float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
         for_each_loaded(n, zf, [&](int, float4 t) { if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t); });
-        if (n <= kRankMax) {
-            int perm[kRankMax];
+        if (n <= kBigCol) {                    // longer columns up to kWarpCol take the warp path
+            int perm[kBigCol];
             rank_order(z.T, b, n, perm);
             for_each_loaded(n, [&](int r) { return zn(perm[r]); },
                             [&](int, float4 t) { if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t); });
@@ -803,6 +791,110 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
     if (BND) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
     st4(R, v, yv);
     if (STATE) c.sptr[v] = b;
+}
+
+// A long column (kBigCol < n <= kWarpCol; the poles of high-valence meshes),
+// by the whole warp: each lane loads its (up to two) slots' records, LAK tails
+// are ranked by id across the warp, SLAK's edge points are independent per
+// slot; the sums run in the order the single-thread path uses, every lane
+// fetching slot k (or the tail of rank r) by shuffle, so the result is the
+// same bit for bit.  No shared memory: the common path keeps its L1.
+template <bool LAK, bool STATE, bool BND>
+__device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict__ P, QState c, SlotScratch z,
+                                            float* __restrict__ R, int compensated, int v, int b, int n)
+{
+    const int lane = threadIdx.x & 31;
+    const float4* Z = z.Z;
+    const bool h0 = lane < n, h1 = lane + 32 < n;
+    const int k0 = b + lane, k1 = b + lane + 32;
+    float4 f0 = f4_zero(), f1 = f4_zero(), n0 = f4_zero(), n1 = f4_zero();   // FP(x) and the neighbour
+    int t0 = INT32_MAX, t1 = INT32_MAX;
+    if (h0) { f0 = __ldg(Z + 2 * (int64_t)k0); n0 = __ldg(Z + 2 * (int64_t)k0 + 1); if (LAK) t0 = __ldg(z.T + k0); }
+    if (h1) { f1 = __ldg(Z + 2 * (int64_t)k1); n1 = __ldg(Z + 2 * (int64_t)k1 + 1); if (LAK) t1 = __ldg(z.T + k1); }
+    const float4 Pv = ldg4(P, v);
+    if (!LAK) {
+        // edge points of C's edges {v, e_out(x)}, ids b..e-1: 0 + (p_v + FP(x))/4 + (Z[2s+1] + Z[2 rot[s]])/4,
+        // FP of slot rot[s] from the lane that holds it
+        const int64_t EPb = (int64_t)d.V + d.N1;
+#pragma unroll
+        for (int el = 0; el < 2; ++el) {
+            const bool h = el ? h1 : h0;
+            const int k = el ? k1 : k0;
+            const int q = h ? __ldg(z.rot + k) - b : 0;
+            const float4 a = shfl4(f0, q & 31), a1 = shfl4(f1, q & 31);
+            if (!h) continue;
+            const float4 fr = q < 32 ? a : a1, nk = el ? n1 : n0, fk = el ? f1 : f0;
+            if (BND && (__ldg(z.bflag + k) & 1)) {
+                st4_cs(R, EPb + k, f4_mul(f4_add(Pv, nk), 0.5f));
+                continue;
+            }
+            const float4 ta = f4_mul(f4_add(Pv, fk), 0.25f);
+            st4_cs(R, EPb + k, f4_add(f4_add(f4_zero(), ta), f4_mul(f4_add(nk, fr), 0.25f)));
+        }
+    }
+    // every lane runs the sums (the same values, by shuffle); lane 0 stores
+    const bool comp = compensated != 0;
+    const float nn = (float)(n * n);
+    float4 yv;
+    if (!LAK) {
+        if (!comp) {
+            float4 acc = f4_zero();
+            for (int k = 0; k < n; ++k) acc = f4_add(acc, col4(n0, n1, k));
+            yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
+            for (int k = 0; k < n; ++k) yv = f4_add(yv, f4_div(col4(f0, f1, k), nn));
+        } else {
+            float4 sh = f4_zero(), sl = f4_zero();
+            for (int k = 0; k < n; ++k) dd_acc(sh, sl, col4(n0, n1, k));
+            for (int k = 0; k < n; ++k) dd_acc(sh, sl, col4(f0, f1, k));
+            yv = vp_finish(sh, sl, Pv, n);
+        }
+    } else {
+        int r0, r1;
+        rank_of(n, t0, t1, r0, r1);                                  // tails in ascending id
+        float4 acc = f4_zero(), sh = f4_zero(), sl = f4_zero();
+        for (int k = 0; k < n; ++k) {
+            const float4 t = col4(f0, f1, k);
+            if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t);
+        }
+        for (int r = 0; r < n; ++r) {
+            int src, el;
+            slot_of_rank(r, h0, h1, r0, r1, src, el);
+            const float4 t = shfl4(el ? n1 : n0, src);
+            if (comp) dd_acc(sh, sl, t); else acc = f4_add(acc, t);
+        }
+        if (comp) yv = vp_finish(sh, sl, Pv, n);
+        else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
+    }
+    if (lane == 0) {
+        if (BND) yv = boundary_vertex<LAK>(P, z, b, b + n, Pv, yv);
+        st4(R, v, yv);
+        if (STATE) c.sptr[v] = b;
+    }
+}
+
+// G3: one thread per vertex v of P.  Its column's records (written by k_g1 at
+// the column's slots) are contiguous, so the vertex point and, for SLAK, the
+// edge points of C's edges {v, e_out(x)} (ids = the slots) stream.  With a
+// boundary (BND), an edge {v, e_out(x)} without a twin gets the midpoint.
+// Columns longer than kBigCol go to their warp (g3_warp_column).
+template <bool LAK, bool STATE, int BS, bool BND = false>
+__global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
+                                           SlotScratch z, float* __restrict__ R, int compensated)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (STATE && v == d.V1) c.sptr[d.V] = d.N;
+    const bool valid = v < d.V1;
+    int b = 0, n = 0;
+    if (valid) { b = __ldg(p.sptr + v); n = __ldg(p.sptr + v + 1) - b; }
+    const bool big = valid && n > kBigCol && n <= kWarpCol;
+    if (valid && !big) g3_vertex<LAK, STATE, BND>(d, P, c, z, R, compensated, v, b, n);
+    unsigned m = __ballot_sync(0xffffffffu, big);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        g3_warp_column<LAK, STATE, BND>(d, P, c, z, R, compensated, __shfl_sync(0xffffffffu, v, src),
+                                        __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
+    }
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -289,17 +289,12 @@ __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __re
     }
 }
 
-// LAK edge ids: ascending (max, min); H = (half-edge min->max, half-edge max->min)
-__global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                           const int* __restrict__ snext, const int* __restrict__ sprev,
-                           const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
-                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
-                           int li)
+// LAK edge ids of one vertex's column on its own thread
+__device__ __forceinline__ void eids_lak_vertex(const int* __restrict__ sc, const int* __restrict__ snext,
+                                                const int* __restrict__ sprev, const int* __restrict__ sprevc,
+                                                const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                                                int2* __restrict__ H, DevStatus* st, int v, int b, int e)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    check_level(v, eptr, V, Ecap, bcount, B, st, li);
-    if (v >= V) return;
-    const int b = sptr[v], e = sptr[v + 1];
     int id = eptr[v], last = -1;
     while (true) {
         int x = INT32_MAX, s = b;
@@ -330,6 +325,92 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
         H[id] = make_int2(cxv, cvx);
         ++id;
         last = x;
+    }
+}
+
+// a long column (kBigCol < n <= kWarpCol) by its warp.  The distinct smaller
+// neighbours are the snext values < v (distinct) plus the sprev values < v not
+// among them; each of a lane's (up to two) slots ranks its values among those,
+// reading the column by shuffle, then writes its own corners' edge ids and
+// their halves of H (-1 for the half whose half-edge is missing) -- the ids
+// and H the serial ascending walk assigns.
+__device__ __noinline__ void eids_lak_warp(const int* __restrict__ sc, const int* __restrict__ snext,
+                                           const int* __restrict__ sprev, const int* __restrict__ sprevc,
+                                           const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                                           int2* __restrict__ H, DevStatus* st, int v, int b, int n)
+{
+    const int lane = threadIdx.x & 31;
+    const bool h0 = lane < n, h1 = lane + 32 < n;
+    const int sn0 = h0 ? __ldg(snext + b + lane) : INT32_MAX, sn1 = h1 ? __ldg(snext + b + lane + 32) : INT32_MAX;
+    const int sp0 = h0 ? __ldg(sprev + b + lane) : INT32_MAX, sp1 = h1 ? __ldg(sprev + b + lane + 32) : INT32_MAX;
+    // fn: my snext value is also a prev; fp: my prev value is also a next
+    int fn0 = 0, fn1 = 0, fp0 = 0, fp1 = 0;
+    for (int j = 0; j < n; ++j) {
+        const int y = col1(sp0, sp1, j), x = col1(sn0, sn1, j);
+        fn0 |= y == sn0; fn1 |= y == sn1;
+        fp0 |= x == sp0; fp1 |= x == sp1;
+    }
+    // rank of value u among the distinct values < v: next values below u, and
+    // prev values below u that are not next values
+    int rn0 = 0, rn1 = 0, rp0 = 0, rp1 = 0;
+    for (int j = 0; j < n; ++j) {
+        const int x = col1(sn0, sn1, j), y = col1(sp0, sp1, j);
+        const int only = !__shfl_sync(0xffffffffu, j < 32 ? fp0 : fp1, j & 31);
+        rn0 += (x < sn0) + ((y < sn0) & only); rn1 += (x < sn1) + ((y < sn1) & only);
+        rp0 += (x < sp0) + ((y < sp0) & only); rp1 += (x < sp1) + ((y < sp1) & only);
+    }
+    const int base = eptr[v];
+    int* Hi = reinterpret_cast<int*>(H);
+#pragma unroll
+    for (int el = 0; el < 2; ++el) {
+        if (!(el ? h1 : h0)) continue;
+        const int k = b + lane + 32 * el;
+        const int u = el ? sn1 : sn0, w = el ? sp1 : sp0;
+        if (u < v) {
+            const int id = base + (el ? rn1 : rn0);
+            if (id >= Ecap) set_error(st, 4, v);
+            else {
+                const int c = __ldg(sc + k);
+                eid[c] = id;
+                Hi[2 * id + 1] = c;
+                if (!(el ? fn1 : fn0)) Hi[2 * id] = -1;
+            }
+        }
+        if (w < v) {
+            const int id = base + (el ? rp1 : rp0);
+            if (id >= Ecap) set_error(st, 4, v);
+            else {
+                const int c = __ldg(sprevc + k);
+                eid[c] = id;
+                Hi[2 * id] = c;
+                if (!(el ? fp1 : fp0)) Hi[2 * id + 1] = -1;
+            }
+        }
+    }
+}
+
+// LAK edge ids: ascending (max, min); H = (half-edge min->max, half-edge
+// max->min), -1 where one is missing.  Columns longer than kBigCol go to
+// their warp.
+__global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                           const int* __restrict__ snext, const int* __restrict__ sprev,
+                           const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
+                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
+                           int li)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    check_level(v, eptr, V, Ecap, bcount, B, st, li);
+    const bool valid = v < V;
+    int b = 0, n = 0;
+    if (valid) { b = sptr[v]; n = sptr[v + 1] - b; }
+    const bool big = valid && n > kBigCol && n <= kWarpCol;
+    if (valid && !big) eids_lak_vertex(sc, snext, sprev, sprevc, eptr, Ecap, eid, H, st, v, b, b + n);
+    unsigned m = __ballot_sync(0xffffffffu, big);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        eids_lak_warp(sc, snext, sprev, sprevc, eptr, Ecap, eid, H, st, __shfl_sync(0xffffffffu, v, src),
+                      __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
     }
 }
 
@@ -423,18 +504,32 @@ __global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __
     st4_cs(EP, e, r);
 }
 
-// SLAK vertex point: vertexSum (:634-652) then the face-point scatter of
-// facepointSum[Quad] (:654-686) in ascending corner order; a boundary vertex
-// becomes 3/4 p + 1/8 next + 1/8 prev (correctBoundaryS1/S2, :688-740).
-template <bool QUAD>
-__global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                          const int* __restrict__ snext, const int* __restrict__ sprev,
-                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
-                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
+// SLAK boundary vertex: 3/4 p + 1/8 next (first out-boundary slot) + 1/8 prev
+// (first in-boundary slot); y unchanged when v has no boundary slot
+__device__ __forceinline__ float4 vp_slak_boundary(const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                   const int* __restrict__ sflag, const float* __restrict__ P,
+                                                   int v, int b, int e, float4 y)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    int sb = -1, si = -1;
+    for (int s = b; s < e; ++s) {
+        int f = sflag[s];
+        if ((f & SF_BOUT) && sb < 0) sb = s;
+        if ((f & SF_BIN) && si < 0) si = s;
+    }
+    if (sb >= 0) y = f4_add(f4_mul(ldg4(P, v), 0.75f), f4_mul(ldg4(P, snext[sb]), 0.125f));
+    if (si >= 0) y = f4_add(y, f4_mul(ldg4(P, sprev[si]), 0.125f));
+    return y;
+}
+
+// SLAK vertex point of one vertex on its own thread
+template <bool QUAD>
+__device__ __forceinline__ void vp_slak_vertex(Faces<QUAD> fc, const int* __restrict__ sc,
+                                               const int* __restrict__ snext, const int* __restrict__ sprev,
+                                               const int* __restrict__ sflag, int boundary,
+                                               const float* __restrict__ P, const float* __restrict__ FP,
+                                               float* __restrict__ R, int compensated, int v, int b, int n)
+{
+    const int e = b + n;
     const float nn = (float)(n * n);
     float4 y;
     const auto nbr = [&](int k) { return ldg4(P, __ldg(snext + b + k)); };
@@ -454,41 +549,111 @@ __global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, c
         for_each_loaded(n, fpt, [&](int, float4 t) { dd_acc(sh, sl, t); });
         y = vp_finish(sh, sl, ldg4(P, v), n);
     }
-    if (boundary) {
-        int sb = -1, si = -1;
-        for (int s = b; s < e; ++s) {
-            int f = sflag[s];
-            if ((f & SF_BOUT) && sb < 0) sb = s;
-            if ((f & SF_BIN) && si < 0) si = s;
-        }
-        if (sb >= 0)
-            y = f4_add(f4_mul(ldg4(P, v), 0.75f), f4_mul(ldg4(P, snext[sb]), 0.125f));
-        if (si >= 0) y = f4_add(y, f4_mul(ldg4(P, sprev[si]), 0.125f));
-    }
+    if (boundary) y = vp_slak_boundary(snext, sprev, sflag, P, v, b, e, y);
     st4(R, v, y);
 }
 
-// LAK vertex point ((sum fp + sum p_tail) / n + p (n - 2)) / n with the face
-// points in corner order and the incoming tails in ascending vertex id
-// (spmv_right_mapped_f4 over M then over F, LAKCatmullClarkImpl.cu:200-221);
-// boundary vertex 3/4 p + 1/8 p_other per boundary edge in edge-id order
-// (prepare/calculateExternalVertexUpdate, LAKCatmullClarkKernels.cuh:464-511).
+// a long column (kBigCol < n <= kWarpCol) by its warp: each lane loads its (up
+// to two) slots; the sums run in column order with every lane fetching slot k
+// by shuffle; lane 0 stores
 template <bool QUAD>
-__global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                         const int* __restrict__ snext, const int* __restrict__ sprev,
-                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
-                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
-                         const float* __restrict__ FP, float* __restrict__ R, int compensated)
+__device__ __noinline__ void vp_slak_warp(Faces<QUAD> fc, const int* __restrict__ sc,
+                                          const int* __restrict__ snext, const int* __restrict__ sprev,
+                                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                                          const float* __restrict__ FP, float* __restrict__ R, int compensated,
+                                          int v, int b, int n)
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const int b = sptr[v], e = sptr[v + 1], n = e - b;
+    const int lane = threadIdx.x & 31;
+    float4 a0 = f4_zero(), a1 = f4_zero(), f0 = f4_zero(), f1 = f4_zero();    // neighbour, face point
+    if (lane < n) { a0 = ldg4(P, __ldg(snext + b + lane)); f0 = ldg4(FP, fc.face(__ldg(sc + b + lane))); }
+    if (lane + 32 < n) { a1 = ldg4(P, __ldg(snext + b + lane + 32)); f1 = ldg4(FP, fc.face(__ldg(sc + b + lane + 32))); }
+    const float nn = (float)(n * n);
+    float4 y;
+    if (!compensated) {
+        float4 acc = f4_zero();
+        for (int k = 0; k < n; ++k) acc = f4_add(acc, col4(a0, a1, k));
+        y = f4_add(f4_div(acc, nn), f4_div(f4_mul(ldg4(P, v), (float)(n - 2)), (float)n));
+        for (int k = 0; k < n; ++k) y = f4_add(y, f4_div(col4(f0, f1, k), nn));
+    } else {
+        float4 sh = f4_zero(), sl = f4_zero();
+        for (int k = 0; k < n; ++k) dd_acc(sh, sl, col4(a0, a1, k));
+        for (int k = 0; k < n; ++k) dd_acc(sh, sl, col4(f0, f1, k));
+        y = vp_finish(sh, sl, ldg4(P, v), n);
+    }
+    if (lane == 0) {
+        if (boundary) y = vp_slak_boundary(snext, sprev, sflag, P, v, b, b + n, y);
+        st4(R, v, y);
+    }
+}
+
+// SLAK vertex point: vertexSum (:634-652) then the face-point scatter of
+// facepointSum[Quad] (:654-686) in ascending corner order; a boundary vertex
+// becomes 3/4 p + 1/8 next + 1/8 prev (correctBoundaryS1/S2, :688-740).
+// Columns longer than kBigCol go to their warp.
+template <bool QUAD>
+__global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                          const int* __restrict__ snext, const int* __restrict__ sprev,
+                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = v < V;
+    int b = 0, n = 0;
+    if (valid) { b = sptr[v]; n = sptr[v + 1] - b; }
+    const bool big = valid && n > kBigCol && n <= kWarpCol;
+    if (valid && !big) vp_slak_vertex<QUAD>(fc, sc, snext, sprev, sflag, boundary, P, FP, R, compensated, v, b, n);
+    unsigned m = __ballot_sync(0xffffffffu, big);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        vp_slak_warp<QUAD>(fc, sc, snext, sprev, sflag, boundary, P, FP, R, compensated,
+                           __shfl_sync(0xffffffffu, v, src), __shfl_sync(0xffffffffu, b, src),
+                           __shfl_sync(0xffffffffu, n, src));
+    }
+}
+
+// LAK boundary vertex: 3/4 p + 1/8 p_other per boundary edge in edge-id order;
+// y unchanged when v has no boundary slot
+__device__ __forceinline__ float4 vp_lak_boundary(const int* __restrict__ sc, const int* __restrict__ snext,
+                                                  const int* __restrict__ sprev, const int* __restrict__ sprevc,
+                                                  const int* __restrict__ sflag, const int* __restrict__ eid,
+                                                  const float* __restrict__ P, int v, int b, int e, float4 y)
+{
+    bool any = false;
+    for (int s = b; s < e; ++s) any |= (sflag[s] & (SF_BOUT | SF_BIN)) != 0;
+    if (!any) return y;
+    y = f4_mul(ldg4(P, v), 0.75f);
+    int lastid = -1;
+    while (true) {
+        int best = INT32_MAX, other = -1;
+        for (int s = b; s < e; ++s) {
+            int f = sflag[s];
+            if (f & SF_BOUT) { int id = eid[sc[s]]; if (id > lastid && id < best) { best = id; other = snext[s]; } }
+            if (f & SF_BIN) { int id = eid[sprevc[s]]; if (id > lastid && id < best) { best = id; other = sprev[s]; } }
+        }
+        if (best == INT32_MAX) break;
+        y = f4_add(y, f4_mul(ldg4(P, other), 0.125f));
+        lastid = best;
+    }
+    return y;
+}
+
+// LAK vertex point of one vertex on its own thread
+template <bool QUAD>
+__device__ __forceinline__ void vp_lak_vertex(Faces<QUAD> fc, const int* __restrict__ sc,
+                                              const int* __restrict__ snext, const int* __restrict__ sprev,
+                                              const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                                              const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                                              const float* __restrict__ FP, float* __restrict__ R, int compensated,
+                                              int v, int b, int n)
+{
+    const int e = b + n;
     const auto fpt = [&](int k) { return ldg4(FP, fc.face(__ldg(sc + b + k))); };
     float4 acc = f4_zero();
     for_each_loaded(n, fpt, [&](int, float4 t) { acc = f4_add(acc, t); });
     // the tails (distinct neighbours) in ascending id
-    int perm[kRankMax];
-    const bool ranked = n <= kRankMax;
+    int perm[kBigCol];
+    const bool ranked = n <= kBigCol;      // longer columns up to kWarpCol take the warp path
     if (ranked) rank_order(sprev, b, n, perm);
     const auto tail = [&](int r) { return ldg4(P, __ldg(sprev + b + perm[r])); };
     if (ranked) {
@@ -524,26 +689,84 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
         }
         y = vp_finish(sh, sl, ldg4(P, v), n);
     }
-    if (boundary) {
-        bool any = false;
-        for (int s = b; s < e; ++s) any |= (sflag[s] & (SF_BOUT | SF_BIN)) != 0;
-        if (any) {
-            y = f4_mul(ldg4(P, v), 0.75f);
-            int lastid = -1;
-            while (true) {
-                int best = INT32_MAX, other = -1;
-                for (int s = b; s < e; ++s) {
-                    int f = sflag[s];
-                    if (f & SF_BOUT) { int id = eid[sc[s]]; if (id > lastid && id < best) { best = id; other = snext[s]; } }
-                    if (f & SF_BIN) { int id = eid[sprevc[s]]; if (id > lastid && id < best) { best = id; other = sprev[s]; } }
-                }
-                if (best == INT32_MAX) break;
-                y = f4_add(y, f4_mul(ldg4(P, other), 0.125f));
-                lastid = best;
-            }
-        }
-    }
+    if (boundary) y = vp_lak_boundary(sc, snext, sprev, sprevc, sflag, eid, P, v, b, e, y);
     st4(R, v, y);
+}
+
+// a long column (kBigCol < n <= kWarpCol) by its warp: each lane loads its (up
+// to two) slots, the tails are ranked by id across the warp, and the sums run
+// in the fixed order with every lane fetching by shuffle; lane 0 stores
+template <bool QUAD>
+__device__ __noinline__ void vp_lak_warp(Faces<QUAD> fc, const int* __restrict__ sc,
+                                         const int* __restrict__ snext, const int* __restrict__ sprev,
+                                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                                         const float* __restrict__ FP, float* __restrict__ R, int compensated,
+                                         int v, int b, int n)
+{
+    const int lane = threadIdx.x & 31;
+    const bool h0 = lane < n, h1 = lane + 32 < n;
+    float4 f0 = f4_zero(), f1 = f4_zero(), p0 = f4_zero(), p1 = f4_zero();    // face point, tail position
+    int t0 = INT32_MAX, t1 = INT32_MAX;                                     // tail ids
+    if (h0) { f0 = ldg4(FP, fc.face(__ldg(sc + b + lane))); t0 = __ldg(sprev + b + lane); p0 = ldg4(P, t0); }
+    if (h1) { f1 = ldg4(FP, fc.face(__ldg(sc + b + lane + 32))); t1 = __ldg(sprev + b + lane + 32); p1 = ldg4(P, t1); }
+    int r0, r1;
+    rank_of(n, t0, t1, r0, r1);
+    float4 y;
+    if (!compensated) {
+        float4 acc = f4_zero();
+        for (int k = 0; k < n; ++k) acc = f4_add(acc, col4(f0, f1, k));
+        for (int r = 0; r < n; ++r) {
+            int src, el;
+            slot_of_rank(r, h0, h1, r0, r1, src, el);
+            acc = f4_add(acc, shfl4(el ? p1 : p0, src));
+        }
+        float4 pn = f4_mul(ldg4(P, v), __fadd_rn((float)n, -2.0f));
+        y = f4_div_z(f4_add(f4_div_z(acc, (float)n), pn), (float)n);
+    } else {
+        float4 sh = f4_zero(), sl = f4_zero();
+        for (int k = 0; k < n; ++k) dd_acc(sh, sl, col4(f0, f1, k));
+        for (int r = 0; r < n; ++r) {
+            int src, el;
+            slot_of_rank(r, h0, h1, r0, r1, src, el);
+            dd_acc(sh, sl, shfl4(el ? p1 : p0, src));
+        }
+        y = vp_finish(sh, sl, ldg4(P, v), n);
+    }
+    if (lane == 0) {
+        if (boundary) y = vp_lak_boundary(sc, snext, sprev, sprevc, sflag, eid, P, v, b, b + n, y);
+        st4(R, v, y);
+    }
+}
+
+// LAK vertex point ((sum fp + sum p_tail) / n + p (n - 2)) / n with the face
+// points in corner order and the incoming tails in ascending vertex id
+// (spmv_right_mapped_f4 over M then over F, LAKCatmullClarkImpl.cu:200-221);
+// boundary vertex 3/4 p + 1/8 p_other per boundary edge in edge-id order
+// (prepare/calculateExternalVertexUpdate, LAKCatmullClarkKernels.cuh:464-511).
+// Columns longer than kBigCol go to their warp.
+template <bool QUAD>
+__global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                         const int* __restrict__ snext, const int* __restrict__ sprev,
+                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                         const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = v < V;
+    int b = 0, n = 0;
+    if (valid) { b = sptr[v]; n = sptr[v + 1] - b; }
+    const bool big = valid && n > kBigCol && n <= kWarpCol;
+    if (valid && !big)
+        vp_lak_vertex<QUAD>(fc, sc, snext, sprev, sprevc, sflag, eid, boundary, P, FP, R, compensated, v, b, n);
+    unsigned m = __ballot_sync(0xffffffffu, big);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        vp_lak_warp<QUAD>(fc, sc, snext, sprev, sprevc, sflag, eid, boundary, P, FP, R, compensated,
+                          __shfl_sync(0xffffffffu, v, src), __shfl_sync(0xffffffffu, b, src),
+                          __shfl_sync(0xffffffffu, n, src));
+    }
 }
 
 }  // namespace slak

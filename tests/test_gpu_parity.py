@@ -12,7 +12,7 @@ import oracle
 from slak_b200 import api, meshgen
 from slak_b200.mesh import LAK, QUAD, SLAK
 
-from meshes import bowtie, open_grid, open_mixed, small_set
+from meshes import bowtie, fan_disk, open_grid, open_mixed, small_set
 
 pytestmark = pytest.mark.gpu
 
@@ -228,3 +228,28 @@ def test_bowtie_slak_differs_only_where_the_reference_races():
         ref = oracle.subdivide(mesh, lv, SLAK)
         assert np.array_equal(fast.ids, ref.ids) and np.array_equal(fast.ids, gen.ids)
         assert _bits_equal(fast.verts, gen.verts)
+
+
+HIGH_VALENCE = [("cyl24", lambda: meshgen.capped_cylinder(24, 4, 0.001, seed=6), 4),
+                ("cyl64", lambda: meshgen.capped_cylinder(64, 3, 0.001, seed=8), 3),
+                ("cyl80", lambda: meshgen.capped_cylinder(80, 3, 0.001, seed=7), 3),
+                ("fan40", lambda: fan_disk(40), 4),
+                ("fan70", lambda: fan_disk(70), 3)]
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name,make,levels", HIGH_VALENCE, ids=[c[0] for c in HIGH_VALENCE])
+def test_high_valence_columns(name, make, levels, scheme):
+    """Columns of 17-64 slots are taken by a whole warp (k_eids_lak, k_vp_*,
+    k_g3), longer ones by one thread: both bit-exact with the oracle, closed
+    poles and a boundary fan centre, plain and compensated."""
+    mesh = make()
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    got, ref = _check(mesh, levels, scheme)
+    assert _bits_equal(got.verts, ref.verts)
+    gen = api.subdivide(mesh, levels, scheme, api._abi.PLAN_GENERAL)
+    assert np.array_equal(got.ids, gen.ids) and _bits_equal(got.verts, gen.verts)
+    a = api.subdivide(mesh, levels, scheme, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(mesh, levels, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+    assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
