@@ -113,6 +113,23 @@ struct Lc {
     int err = 0;
     std::vector<cudaEvent_t>* ev = nullptr;   // timing: one event after every launch (ev[0] before the first)
     std::vector<KernelRec>* recs = nullptr;
+    // independent kernels of a level on side streams (fork / join by events);
+    // off while timing (per-launch events need one stream) and when debugging
+    bool conc = false;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t cev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // side stream k waits for the work enqueued so far on s
+    void fork(int k)
+    {
+        cudaEventRecord(cev[k], s);
+        cudaStreamWaitEvent(side[k], cev[k], 0);
+    }
+    // s waits for side stream k
+    void join(int k)
+    {
+        cudaEventRecord(cev[2 + k], side[k]);
+        cudaStreamWaitEvent(s, cev[2 + k], 0);
+    }
     void after(const char* name, int n = 1, int64_t bytes = 0)
     {
         *nl += n;
@@ -173,6 +190,10 @@ struct slak_plan {
     // per-launch timing (SLAK_PLAN_TIMING)
     std::vector<cudaEvent_t> ev;
     std::vector<KernelRec> recs;
+    // side streams and fork / join events for a level's independent kernels
+    // (standalone plans; a batch overlaps whole meshes instead)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t cev[4] = {nullptr, nullptr, nullptr, nullptr};
     // creases (slak_plan_create_creased): a snapshot of the pairs and
     // sharpness, the crease list of each level that has a live crease
     // (ncrease << level entries), the base vertices' crease edges (CSR) and
@@ -293,15 +314,19 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
         k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
                                                       bcount, (int)L.B, li);
     lc.after("k_eids");
+    // the refined quads (side stream 0) need only the edge ids; the positions
+    // (k_fp, then k_ep on side stream 1 beside k_vp) need the face points
+    if (lc.conc) lc.fork(0);
+    cudaStream_t s_ref = lc.conc ? lc.side[0] : str;
     if (lak)
-        k_refine<QUAD, true><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
-                                                              reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
-                                                              reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
-                                                              nullptr);
+        k_refine<QUAD, true><<<grid_for(N), kBlock, 0, s_ref>>>(fc, L.ids, s.eid, N, V, F,
+                                                                reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
+                                                                reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
+                                                                nullptr);
     else
-        k_refine<QUAD, false><<<grid_for(N), kBlock, 0, str>>>(fc, L.ids, s.eid, N, V, F,
-                                                               reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
-                                                               s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
+        k_refine<QUAD, false><<<grid_for(N), kBlock, 0, s_ref>>>(fc, L.ids, s.eid, N, V, F,
+                                                                 reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
+                                                                 s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
     lc.after("k_refine");
     float* R = L.o_verts;
     float* FPo = R + 4 * (size_t)V;
@@ -313,10 +338,12 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     else
         k_fp_seq<QUAD, false><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
     lc.after("k_fp");
+    if (lc.conc) lc.fork(1);
+    cudaStream_t s_ep = lc.conc ? lc.side[1] : str;
     if (lak)
-        k_ep<QUAD, true><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        k_ep<QUAD, true><<<grid_for(E), kBlock, 0, s_ep>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
     else
-        k_ep<QUAD, false><<<grid_for(E), kBlock, 0, str>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        k_ep<QUAD, false><<<grid_for(E), kBlock, 0, s_ep>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
     lc.after("k_ep");
     const int bnd = L.B > 0;
     if (lak)
@@ -326,6 +353,7 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
         k_vp_slak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
                                                          L.verts, FPo, R, compensated);
     lc.after("k_vp");
+    if (lc.conc) { lc.join(0); lc.join(1); }
 }
 
 // One fast level: C = L (refined from its parent level Pl, whose state is
@@ -350,13 +378,16 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     });
     lc.after("k_g1", 1, (PQ ? g1b + g2b : g1b) + (optr ? 4 * (L.N + 1) + 16 * L.N : 0));
     if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
-        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, str>>>(d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts,
-                                                              comp ? 1 : 0);
+        // k_gf, k_g2 and k_g3 read only k_g1's records and the level's inputs and
+        // write disjoint outputs: with side streams they run side by side
+        if (lc.conc) { lc.fork(0); lc.fork(1); }
+        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, lc.conc ? lc.side[0] : str>>>(
+            d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts, comp ? 1 : 0);
         lc.after("k_gf");
         with_block(L.bs[1], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            k_g2<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
-                                                                             L.out_state, L.o_verts);
+            k_g2<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, lc.conc ? lc.side[1] : str>>>(
+                d, pf, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
         });
         lc.after("k_g2", 1, g2b);
     }
@@ -371,6 +402,7 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
         scan_exclusive(L.slots.bscan, L.out_state.brank, Pl.N, L.scan_tmp, str, &nl);
         lc.after("scan(boundary)", (int)nl);
     }
+    if (!PQ && lc.conc) { lc.join(0); lc.join(1); }
 }
 
 template <bool PQ, bool BND>
@@ -449,6 +481,11 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
 {
     int64_t nl = 0;
     Lc lc{str, &nl, p->debug, 0};
+    if (p->side[0] && !(p->flags & SLAK_PLAN_TIMING) && !p->debug) {
+        lc.conc = true;
+        for (int k = 0; k < 2; ++k) lc.side[k] = p->side[k];
+        for (int k = 0; k < 4; ++k) lc.cev[k] = p->cev[k];
+    }
     if (p->flags & SLAK_PLAN_TIMING) {
         if (p->ev.empty()) {
             p->ev.resize(512);
@@ -493,6 +530,10 @@ void free_plan_memory(slak_plan* p)
 {
     for (auto& e : p->ev) cudaEventDestroy(e);
     p->ev.clear();
+    for (auto& e : p->cev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+    for (auto& st : p->side)
+        if (st) { cudaStreamDestroy(st); st = nullptr; }
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     p->gexec = nullptr;
     if (p->arena && p->arena_owned) cudaFree(p->arena);
@@ -959,6 +1000,11 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
     }
     rc = probe_level0(p, p->lv[0], str, probe_mem);
     if (rc == SLAK_OK) rc = plan_levels(p);
+    if (rc == SLAK_OK) {              // side streams for the levels' independent kernels
+        for (int k = 0; k < 2 && ce == cudaSuccess; ++k) ce = cudaStreamCreateWithFlags(&p->side[k], cudaStreamNonBlocking);
+        for (int k = 0; k < 4 && ce == cudaSuccess; ++k) ce = cudaEventCreateWithFlags(&p->cev[k], cudaEventDisableTiming);
+        if (ce != cudaSuccess) rc = cuda_status(ce);
+    }
     if (rc == SLAK_OK && ncrease > 0) rc = plan_crease_setup(p, csharp, ncrease, str);
     if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
     Carver dry(nullptr);
