@@ -123,15 +123,11 @@ __device__ __forceinline__ void for_each_loaded(int n, Load load, Add add)
 }
 
 // ---------------------------------------------------------------- ordering
-// The slots k = 0..n-1 of key[b..b+n) in ascending key order (equal keys by
-// slot): perm[r] = the slot of rank r.  n^2 independent compares, instead of
-// n selection passes that each wait for the previous minimum; for columns of
-// up to kRankMax slots (high-valence vertices; shorter ones stay in registers).
-constexpr int kRankMax = 64;
-
 // Columns longer than kBigCol slots (and up to kWarpCol) are taken by their
-// whole warp: loads and ranks in parallel into shared memory, then one lane
-// adds the sums in the fixed order (same bits as the single-thread paths).
+// whole warp: each lane holds two slots, ranks and loads run in parallel, and
+// the sums run in the fixed order by shuffle (same bits as the single-thread
+// paths, no shared memory).  Shorter columns, and longer ones, stay on one
+// thread.
 constexpr int kBigCol = 16;
 constexpr int kWarpCol = 64;
 
@@ -166,6 +162,10 @@ __device__ __forceinline__ void slot_of_rank(int r, bool h0, bool h1, int r0, in
     el = m0 ? 0 : 1;
     src = __ffs(m0 ? m0 : m1) - 1;
 }
+// The slots k = 0..n-1 of key[b..b+n) in ascending key order (equal keys by
+// slot): perm[r] = the slot of rank r.  n^2 independent compares, instead of
+// n selection passes that each wait for the previous minimum; for one thread's
+// columns of 5 to kBigCol slots (shorter ones are ranked in registers).
 __device__ __forceinline__ void rank_order(const int* __restrict__ key, int b, int n, int* perm)
 {
     for (int k = 0; k < n; ++k) {
