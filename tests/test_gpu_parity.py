@@ -253,3 +253,30 @@ def test_high_valence_columns(name, make, levels, scheme):
     a = api.subdivide(mesh, levels, scheme, api._abi.PLAN_COMPENSATED)
     b = api.subdivide(mesh, levels, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
     assert np.array_equal(a.ids, b.ids) and _bits_equal(a.verts, b.verts)
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+def test_run_to_run_identical(scheme):
+    """Unlike the reference (atomic slot and edge numbering, float atomics),
+    repeated executions give the same bytes: five eager and five graph
+    executions of a plan whose levels fork kernels onto side streams."""
+    import hashlib
+    import torch
+    for mesh, levels in ((meshgen.mixed_torus(64, 48, 0.05, 0.03, 0.005, seed=4), 3),
+                         (meshgen.capped_cylinder(64, 8, 0.001, seed=6), 3)):
+        if scheme == LAK and mesh.ptr is None:
+            mesh = mesh.with_quad_ptr()
+        dm = api.DeviceMesh.from_host(mesh)
+        s = torch.cuda.Stream()
+        digests = set()
+        for flags in (0, api._abi.PLAN_GRAPH):
+            plan = api.Plan(dm, levels, scheme, flags, stream=s)
+            for _ in range(5):
+                plan.execute(s)
+                plan.check(s)
+                out = plan.output().to_host()
+                torch.cuda.synchronize()
+                h = hashlib.sha256(out.ids.tobytes() + np.asarray(out.verts, np.float32).tobytes()).hexdigest()
+                digests.add(h)
+            plan.close()
+        assert len(digests) == 1
