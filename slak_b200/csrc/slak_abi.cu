@@ -191,9 +191,10 @@ struct slak_plan {
     std::vector<cudaEvent_t> ev;
     std::vector<KernelRec> recs;
     // side streams and fork / join events for a level's independent kernels
-    // (standalone plans; a batch overlaps whole meshes instead)
+    // (a standalone plan owns them; a batch lends its stream slot's)
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t cev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool side_owned = true;
     // creases (slak_plan_create_creased): a snapshot of the pairs and
     // sharpness, the crease list of each level that has a live crease
     // (ncrease << level entries), the base vertices' crease edges (CSR) and
@@ -530,10 +531,14 @@ void free_plan_memory(slak_plan* p)
 {
     for (auto& e : p->ev) cudaEventDestroy(e);
     p->ev.clear();
-    for (auto& e : p->cev)
-        if (e) { cudaEventDestroy(e); e = nullptr; }
-    for (auto& st : p->side)
-        if (st) { cudaStreamDestroy(st); st = nullptr; }
+    for (auto& e : p->cev) {
+        if (e && p->side_owned) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    for (auto& st : p->side) {
+        if (st && p->side_owned) cudaStreamDestroy(st);
+        st = nullptr;
+    }
     if (p->gexec) cudaGraphExecDestroy(p->gexec);
     p->gexec = nullptr;
     if (p->arena && p->arena_owned) cudaFree(p->arena);
@@ -1297,6 +1302,11 @@ struct slak_batch {
     size_t out_bytes = 0, arena_bytes = 0;
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> fork, join;
+    // per stream slot: two side streams and four events lent to the plans it
+    // runs (a plan records each event and waits on it at once, so plans that
+    // follow one another on a slot can share them)
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> sev;
     cudaGraphExec_t gexec = nullptr;
     DevStatus* h_st = nullptr;                  // pinned, one per mesh
     DevStatus* d_st = nullptr;                  // device, one per mesh (outlives the waves' arenas)
@@ -1316,6 +1326,8 @@ void batch_free(slak_batch* b)
     for (auto* p : b->plans)
         if (p) { free_plan_memory(p); delete p; }
     for (auto s : b->streams) cudaStreamDestroy(s);
+    for (auto s : b->side) cudaStreamDestroy(s);
+    for (auto e : b->sev) cudaEventDestroy(e);
     for (auto e : b->fork) cudaEventDestroy(e);
     for (auto e : b->join) cudaEventDestroy(e);
     if (b->out_mem) cudaFree(b->out_mem);
@@ -1351,7 +1363,14 @@ int batch_enqueue(slak_batch* b, cudaStream_t str)
         for (int k = 0; k < nb; ++k) cudaStreamWaitEvent(b->streams[k], b->fork[w], 0);
         for (size_t j = 0; j < wave.size(); ++j) {
             slak_plan* p = b->plans[wave[j]];
-            int rc = enqueue_all(p, b->streams[j % nb]);
+            const int k = (int)(j % nb);
+            if (!b->side.empty()) {
+                p->side[0] = b->side[2 * k];
+                p->side[1] = b->side[2 * k + 1];
+                for (int i = 0; i < 4; ++i) p->cev[i] = b->sev[4 * k + i];
+                p->side_owned = false;
+            }
+            int rc = enqueue_all(p, b->streams[k]);
             if (rc != SLAK_OK) return rc;
             nl += p->launches;
         }
@@ -1544,6 +1563,10 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
         for (auto& e : b->join) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
         b->streams.resize(kBatchStreams);
         for (auto& st2 : b->streams) cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+        b->side.resize(2 * kBatchStreams);
+        for (auto& st2 : b->side) cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking);
+        b->sev.resize(4 * kBatchStreams);
+        for (auto& e : b->sev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
         ce = cudaGetLastError();
         if (ce != cudaSuccess) rc = cuda_status(ce);
     }
