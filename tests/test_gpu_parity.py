@@ -280,3 +280,29 @@ def test_run_to_run_identical(scheme):
                 digests.add(h)
             plan.close()
         assert len(digests) == 1
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("flags", [0, api._abi.PLAN_GENERAL])
+def test_degenerate_faces_rejected(scheme, flags):
+    """Inputs the reference does not validate are rejected with
+    SLAK_ERR_BAD_MESH instead of refined into garbage: a face that repeats a
+    vertex (a half-edge v -> v), a face of two corners, decreasing offsets."""
+    from slak_b200.mesh import from_arrays
+    m = meshgen.mixed_torus(12, 10, 0.1, 0.06, 0.005, seed=5)
+    ptr, ids = np.asarray(m.ptr), np.asarray(m.ids).copy()
+    V = np.asarray(m.verts, np.float32)[:, :3]
+    bads = []
+    rep = ids.copy()
+    rep[ptr[3] + 1] = rep[ptr[3]]                                   # repeated vertex in face 3
+    bads.append(from_arrays(ptr, rep, V))
+    short = np.concatenate([[0], ptr[1:] - ptr[1] + 2]).astype(np.int32)   # face 0 of two corners
+    bads.append(from_arrays(short, np.concatenate([ids[:2], ids[ptr[1]:]]), V))
+    dec = m.copy()
+    dec.ptr = ptr.copy()
+    dec.ptr[5], dec.ptr[6] = ptr[6], ptr[5]                         # offsets out of order
+    bads.append(dec)
+    for bad in bads:
+        with pytest.raises(api._abi.SlakError) as e:
+            api.subdivide(bad, 2, scheme, flags)
+        assert e.value.code == api._abi.SLAK_ERR_BAD_MESH
