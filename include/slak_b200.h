@@ -130,6 +130,23 @@ int slak_obj_read_creased(const char* path, slak_mesh* out, slak_creases* crease
 int slak_obj_write_creased(const char* path, const slak_mesh* host_mesh, const slak_creases* creases);
 int slak_obj_free_creases(slak_creases* creases);
 
+/* Corner vertices of a mesh: count vertex ids and count sharpness values. */
+typedef struct slak_corners {
+    int64_t count;
+    int32_t* verts;
+    float* sharpness;
+} slak_corners;
+
+/* As slak_obj_read_creased, and also reads "t corner" tags: ni >= 1 0-based
+ * vertex ids with one sharpness (nf == 1) or one each (nf == ni) (host
+ * arrays, malloc; release with slak_obj_free_corners).  slak_obj_write_sharp
+ * appends the crease lines (creases may be NULL), then one
+ * "t corner 1/1/0 v s" line per corner (corners may be NULL). */
+int slak_obj_read_sharp(const char* path, slak_mesh* out, slak_creases* creases, slak_corners* corners);
+int slak_obj_write_sharp(const char* path, const slak_mesh* host_mesh, const slak_creases* creases,
+                         const slak_corners* corners);
+int slak_obj_free_corners(slak_corners* corners);
+
 /* Frees the current device's cached slak_subdivide workspace.  No counterpart
  * in the reference, whose calls keep nothing between them.  Returns
  * SLAK_ERR_NOT_READY while a call holds the workspace. */
@@ -280,6 +297,26 @@ int slak_plan_create_creased(const slak_mesh* cmesh, int target_level, int schem
 int slak_subdivide_creased(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
                            const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
                            slak_stream_t stream);
+
+/*
+ * Creases and corners (vertex sharpness, the "t corner" tags OBJ::read also
+ * keeps unused).  A vertex of sharpness s takes the corner rule (it keeps its
+ * position) while s - level > 0, blended with its smooth point by
+ * max(min(1, s - level), min(1, mean sharpness of its crease edges)).
+ * corner_verts holds ncorners vertex ids and corner_sharpness their sharpness,
+ * both in device memory.  They are read at creation: an id out of range or a
+ * vertex named twice gives SLAK_ERR_BAD_MESH, and a sharpness that is not
+ * finite gives SLAK_ERR_INVALID_ARG.  The _creased calls are these with no
+ * corners.
+ */
+int slak_plan_create_sharp(const slak_mesh* cmesh, int target_level, int scheme, int flags,
+                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                           const int32_t* corner_verts, const float* corner_sharpness, int64_t ncorners,
+                           slak_stream_t stream, slak_plan** plan);
+int slak_subdivide_sharp(const slak_mesh* cmesh, slak_mesh* rmesh, int target_level, int scheme,
+                         const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                         const int32_t* corner_verts, const float* corner_sharpness, int64_t ncorners,
+                         slak_stream_t stream);
 
 /*
  * Batches: many meshes, each with its own target level, refined by one call

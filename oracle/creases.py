@@ -25,6 +25,11 @@ a live crease:
 A crease pair is matched to the half-edge min -> max of the base mesh; a pair
 on a boundary edge or with s <= 0 does nothing; a pair that is no edge, or an
 interior edge named twice, is an error.
+
+Corners (vertex sharpness, the "t corner" tags): a base vertex of sharpness
+s_v takes the corner rule (p_v) while s_v - level > 0, blended by
+max(min(1, s_v - level), min(1, mean crease sharpness)); an id out of range or
+a vertex named twice is an error.
 """
 from __future__ import annotations
 
@@ -79,9 +84,30 @@ def resolve(mesh, pairs, sharp):
     return np.array(cc, np.int64), np.array(cs, F32), bnd
 
 
-def crease_pass(cur, r, cc, cs, bnd0, last):
+def resolve_corners(V, verts, sharp):
+    """Dense corner sharpness of the base vertices (0: none).  Raises ValueError
+    where the CUDA path rejects the tags (an id out of range, a vertex named
+    twice)."""
+    vcs = np.zeros(V, F32)
+    seen = set()
+    for v, s in zip(np.asarray(verts, np.int64).reshape(-1).tolist(), np.asarray(sharp, F32).tolist()):
+        if v < 0 or v >= V:
+            raise ValueError("corner vertex out of range")
+        if v in seen:
+            raise ValueError("corner vertex named twice")
+        if not np.isfinite(s):
+            raise ValueError("corner sharpness is not finite")
+        seen.add(v)
+        vcs[v] = max(F32(s), F32(0))
+    return vcs
+
+
+def crease_pass(cur, r, cc, cs, bnd0, last, vcs=None, lvl=0):
     """Applies one level's crease rules to the oracle level result ``r`` of the
-    input ``cur`` (in place on r.verts); returns the next level's list."""
+    input ``cur`` (in place on r.verts); returns the next level's list.  With
+    ``vcs`` (corner sharpness of the base vertices), a base vertex whose corner
+    sharpness minus the level is positive takes the corner rule, blended by
+    max(min(1, that), min(1, mean crease sharpness))."""
     quad = cur.type == 1
     ids = np.asarray(cur.ids, np.int64)
     nxt = _next_corner(cur.ptr, ids.size, quad)
@@ -105,12 +131,30 @@ def crease_pass(cur, r, cc, cs, bnd0, last):
     starts = np.flatnonzero(np.r_[True, v[1:] != v[:-1]]) if v.size else np.zeros(0, np.int64)
     ends = np.r_[starts[1:], v.size]
     V0 = bnd0.size
-    for st, en in zip(starts.tolist(), ends.tolist()):
-        vx = int(v[st])
+    groups = {int(v[st]): (st, en) for st, en in zip(starts.tolist(), ends.tolist())}
+    corner = {}
+    if vcs is not None:
+        cv = vcs - F32(lvl)
+        corner = {int(x): cv[x] for x in np.flatnonzero(cv > F32(0)).tolist()}
+    for vx in sorted(set(groups) | set(corner)):
+        st, en = groups.get(vx, (0, 0))
         k = en - st
         ssum = F32(0)
         for t in range(st, en):
             ssum = F32(ssum + sv[t])
+        if vx in corner:
+            wk = F32(0)
+            if k > 0:
+                wk = F32(ssum / F32(k))
+                if wk > F32(1):
+                    wk = F32(1)
+            wc = corner[vx] if corner[vx] < F32(1) else F32(1)
+            w = wc if wc > wk else wk
+            if w >= F32(1):
+                R[vx] = P[vx]
+            else:
+                R[vx] = R[vx] * (F32(1) - w) + P[vx] * w
+            continue
         w = F32(ssum / F32(k))
         if w > F32(1):
             w = F32(1)
@@ -133,12 +177,17 @@ def crease_pass(cur, r, cc, cs, bnd0, last):
     return ncc, ncs
 
 
-def subdivide_creased(mesh, levels: int, scheme: int, pairs, sharp):
+def subdivide_creased(mesh, levels: int, scheme: int, pairs, sharp, corners=None):
     """Oracle levels with the crease pass after each level that has a live
-    crease; returns the last level's Result (positions float32)."""
+    crease or corner; returns the last level's Result (positions float32).
+    ``corners``: None or (vertex ids, sharpness)."""
     nlev = levels if mesh.type == 1 else max(levels, 1)
-    cc, cs, bnd0 = resolve(mesh, pairs, sharp)
+    cc, cs, bnd0 = resolve(mesh, np.asarray(pairs, np.int64).reshape(-1, 2), sharp)
     smax = float(np.max(np.asarray(sharp, F32))) if np.asarray(sharp).size else 0.0
+    vcs = None
+    if corners is not None and np.asarray(corners[1]).size:
+        vcs = resolve_corners(bnd0.size, corners[0], corners[1])
+        smax = max(smax, float(vcs.max()))
     crease_levels = min(nlev, math.ceil(smax)) if smax > 0 else 0
     cur = mesh
     r = None
@@ -146,7 +195,7 @@ def subdivide_creased(mesh, levels: int, scheme: int, pairs, sharp):
         r = level(cur, scheme, poly=(l == 0 and mesh.type != 1))
         r.verts = np.ascontiguousarray(r.verts, F32)
         if l < crease_levels:
-            cc, cs = crease_pass(cur, r, cc, cs, bnd0, last=l + 1 >= crease_levels)
+            cc, cs = crease_pass(cur, r, cc, cs, bnd0, last=l + 1 >= crease_levels, vcs=vcs, lvl=l)
         nxt = _LevelMesh(r)
         nxt.verts64 = None
         cur = nxt

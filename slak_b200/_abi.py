@@ -22,12 +22,19 @@ PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
            "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_obj_read", "slak_obj_write",
            "slak_obj_free", "slak_obj_read_creased", "slak_obj_write_creased", "slak_obj_free_creases",
-           "slak_plan_create", "slak_plan_create_creased", "slak_subdivide_creased",
+           "slak_obj_read_sharp", "slak_obj_write_sharp", "slak_obj_free_corners",
+           "slak_plan_create", "slak_plan_create_creased", "slak_subdivide_creased", "slak_plan_create_sharp",
+           "slak_subdivide_sharp",
            "slak_plan_execute", "slak_plan_status", "slak_plan_output", "slak_plan_release_output",
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
            "slak_plan_destroy", "slak_subdivide_batched", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
            "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
+
+
+class SlakCorners(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int64), ("verts", ctypes.POINTER(ctypes.c_int32)),
+                ("sharpness", ctypes.POINTER(ctypes.c_float))]
 
 
 class SlakCreases(ctypes.Structure):
@@ -94,8 +101,12 @@ def lib():
         L.slak_obj_read_creased.argtypes = [ctypes.c_char_p, P, PC]
         L.slak_obj_write_creased.argtypes = [ctypes.c_char_p, P, PC]
         L.slak_obj_free_creases.argtypes = [PC]
+        PK = ctypes.POINTER(SlakCorners)
+        L.slak_obj_read_sharp.argtypes = [ctypes.c_char_p, P, PC, PK]
+        L.slak_obj_write_sharp.argtypes = [ctypes.c_char_p, P, PC, PK]
+        L.slak_obj_free_corners.argtypes = [PK]
         for n in ("slak_obj_read", "slak_obj_write", "slak_obj_free", "slak_obj_read_creased", "slak_obj_write_creased",
-                  "slak_obj_free_creases"):
+                  "slak_obj_free_creases", "slak_obj_read_sharp", "slak_obj_write_sharp", "slak_obj_free_corners"):
             getattr(L, n).restype = I
         L.slak_workspace_release.argtypes = []
         L.slak_workspace_release.restype = I
@@ -103,6 +114,8 @@ def lib():
         L.slak_plan_create.argtypes = [P, I, I, I, V, ctypes.POINTER(V)]
         L.slak_plan_create_creased.argtypes = [P, I, I, I, V, V, I64, V, ctypes.POINTER(V)]
         L.slak_subdivide_creased.argtypes = [P, P, I, I, V, V, I64, V]
+        L.slak_plan_create_sharp.argtypes = [P, I, I, I, V, V, I64, V, V, I64, V, ctypes.POINTER(V)]
+        L.slak_subdivide_sharp.argtypes = [P, P, I, I, V, V, I64, V, V, I64, V]
         L.slak_plan_execute.argtypes = [V, V]
         L.slak_plan_status.argtypes = [V, V]
         L.slak_plan_output.argtypes = [V, P]
@@ -132,7 +145,8 @@ def lib():
                   "slak_batch_num_waves", "slak_batch_destroy"):
             getattr(L, n).restype = I
         for n in ("slak_subdivide", "slak_mesh_free", "slak_subdivide_level_noalloc", "slak_plan_create",
-                  "slak_plan_create_creased", "slak_subdivide_creased", "slak_plan_execute", "slak_plan_status",
+                  "slak_plan_create_creased", "slak_subdivide_creased", "slak_plan_create_sharp",
+                  "slak_subdivide_sharp", "slak_plan_execute", "slak_plan_status",
                   "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
                   "slak_plan_level_stats", "slak_plan_destroy"):
             getattr(L, n).restype = I

@@ -168,27 +168,45 @@ def _crease_tensors(creases):
     return pairs, sharp
 
 
+def _corner_tensors(corners):
+    """(vertex ids, sharpness) as contiguous int32 (k,) and float32 (k,) CUDA tensors."""
+    torch = _torch()
+    kv, ks = corners
+    kv = torch.as_tensor(np.asarray(kv) if not torch.is_tensor(kv) else kv)
+    ks = torch.as_tensor(np.asarray(ks) if not torch.is_tensor(ks) else ks)
+    kv = kv.to(device="cuda", dtype=torch.int32).reshape(-1).contiguous()
+    ks = ks.to(device="cuda", dtype=torch.float32).reshape(-1).contiguous()
+    if kv.shape[0] != ks.shape[0]:
+        raise ValueError("corners: one sharpness per vertex")
+    return kv, ks
+
+
 class Plan:
     """Sized-once execution of ``levels`` subdivision levels (see slak_plan_create)."""
 
-    def __init__(self, cmesh: DeviceMesh, levels: int, scheme: int, flags: int = 0, stream=None, creases=None):
+    def __init__(self, cmesh: DeviceMesh, levels: int, scheme: int, flags: int = 0, stream=None, creases=None,
+                 corners=None):
         """``creases``: None, or (pairs, sharpness) -- an (m, 2) array of vertex
-        ids and m sharpness values, host arrays or device tensors
-        (slak_plan_create_creased; the plan keeps its own copy)."""
+        ids and m sharpness values; ``corners``: None, or (vertex ids,
+        sharpness).  Host arrays or device tensors (slak_plan_create_sharp; the
+        plan keeps its own copy)."""
         self._cmesh = cmesh            # the plan reads these arrays on every execute
         self._cin = cmesh.as_c()
         h = ctypes.c_void_p()
-        if creases is None:
+        if creases is None and corners is None:
             rc = _abi.lib().slak_plan_create(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
                                              _stream_handle(stream), ctypes.byref(h))
             _abi.check(rc, "slak_plan_create")
         else:
-            pairs, sharp = _crease_tensors(creases)
-            rc = _abi.lib().slak_plan_create_creased(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
-                                                     pairs.data_ptr() if pairs.numel() else None,
-                                                     sharp.data_ptr() if sharp.numel() else None,
-                                                     int(sharp.numel()), _stream_handle(stream), ctypes.byref(h))
-            _abi.check(rc, "slak_plan_create_creased")
+            pairs, sharp = _crease_tensors(creases if creases is not None else (np.zeros((0, 2)), np.zeros(0)))
+            kv, ks = _corner_tensors(corners if corners is not None else (np.zeros(0), np.zeros(0)))
+            rc = _abi.lib().slak_plan_create_sharp(ctypes.byref(self._cin), int(levels), int(scheme), int(flags),
+                                                   pairs.data_ptr() if pairs.numel() else None,
+                                                   sharp.data_ptr() if sharp.numel() else None, int(sharp.numel()),
+                                                   kv.data_ptr() if kv.numel() else None,
+                                                   ks.data_ptr() if ks.numel() else None, int(ks.numel()),
+                                                   _stream_handle(stream), ctypes.byref(h))
+            _abi.check(rc, "slak_plan_create_sharp")
         self._h = h
         self.scheme = scheme
 
@@ -251,12 +269,13 @@ class Plan:
             pass
 
 
-def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0, creases=None) -> HostResult:
+def subdivide(mesh: Mesh, levels: int, scheme: int = SLAK, flags: int = 0, creases=None,
+              corners=None) -> HostResult:
     """Host mesh in, host refined mesh out (H2D, one plan execution, D2H).
-    ``creases``: None or (pairs, sharpness), see Plan."""
+    ``creases`` / ``corners``: None or (ids, sharpness), see Plan."""
     torch = _torch()
     dm = DeviceMesh.from_host(mesh)
-    plan = Plan(dm, levels, scheme, flags, creases=creases)
+    plan = Plan(dm, levels, scheme, flags, creases=creases, corners=corners)
     plan.execute()
     plan.check()
     out = plan.output().to_host()

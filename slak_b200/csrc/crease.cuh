@@ -17,6 +17,8 @@
 //     k == 2: sharp = (3/4 p_v + 1/8 p_o1) + 1/8 p_o2 (o1 < o2, the crease's other ends)
 //     k >= 3: corner, sharp = p_v
 //     result: w >= 1 ? sharp : smooth (1 - w) + sharp w
+//   a corner (vertex sharpness s_v, a base vertex): p_v while s_v - level > 0,
+//     blended by max(min(1, s_v - level), min(1, mean s of its crease edges))
 //   a crease half-edge c (a -> b) of sharpness s > 1 leaves two child
 //   half-edges of sharpness s - 1 in the refined mesh: corner 4c (a -> ep) and
 //   corner 4 next(c) + 3 (ep -> b).
@@ -167,12 +169,14 @@ __global__ void k_crease_verts(Faces<QUAD> fc, int l, int V0, int64_t m, const i
                                const int* __restrict__ cc, const float* __restrict__ cs,
                                const int* __restrict__ vcnt, const int* __restrict__ vptr,
                                const int* __restrict__ inc, const unsigned char* __restrict__ bnd0, CreaseEps eps,
-                               const float* __restrict__ P, float* __restrict__ R)
+                               const float* __restrict__ vcs, const float* __restrict__ P, float* __restrict__ R)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < V0) {
         const int v = (int)idx;
-        if (__ldg(vcnt + v) == 0) return;
+        // corner sharpness left at this level (vertex sharpness decays by one per level)
+        const float cv = vcs ? __fsub_rn(__ldg(vcs + v), (float)l) : 0.0f;
+        if (__ldg(vcnt + v) == 0 && !(cv > 0.0f)) return;
         const int b = __ldg(vptr + v), e = __ldg(vptr + v + 1);
         const int lm = (1 << l) - 1;
         // the live descendants' other ends, visited in ascending id
@@ -199,6 +203,20 @@ __global__ void k_crease_verts(Faces<QUAD> fc, int l, int V0, int64_t m, const i
             ssum = __fadd_rn(ssum, sb);
             ++k;
             last = best;
+        }
+        if (cv > 0.0f) {                // a corner: p_v, blended by max(min(1, cv), min(1, mean s))
+            float wk = 0.0f;
+            if (k > 0) {
+                wk = __fdiv_rn(ssum, (float)k);
+                if (wk > 1.0f) wk = 1.0f;
+            }
+            const float wc = cv < 1.0f ? cv : 1.0f;
+            const float w = wc > wk ? wc : wk;
+            const float4 pv = ldg4(P, v);
+            float4 r = pv;
+            if (!(w >= 1.0f)) r = f4_add(f4_mul(ldg4(R, v), __fsub_rn(1.0f, w)), f4_mul(pv, w));
+            st4(R, v, r);
+            return;
         }
         if (k == 0) return;
         crease_vertex(P, R, v, k, o[0], o[1], ssum, bnd0 != nullptr && bnd0[v] != 0);

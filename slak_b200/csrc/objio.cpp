@@ -15,8 +15,9 @@
 // ints and nf floats); the reference never uses them.  slak_obj_read_creased
 // turns "t crease" tags into crease pairs: the ni >= 2 ints are a chain of
 // 0-based vertex ids v0 v1 ... (edges {v_j, v_j+1}), with one sharpness for
-// the whole chain (nf == 1) or one per edge (nf == ni - 1).  Other tag types
-// are skipped.
+// the whole chain (nf == 1) or one per edge (nf == ni - 1).  slak_obj_read_sharp
+// also reads "t corner" tags: ni >= 1 vertex ids with one sharpness or one
+// each.  Other tag types are skipped.
 #include "slak_b200.h"
 
 #include <algorithm>
@@ -40,6 +41,8 @@ struct Chunk {
     std::vector<int32_t> fi;   // corner vertex indices, 0-based
     std::vector<int32_t> cv;   // crease pairs (2 ids each), when tags are read
     std::vector<float> cs;     // their sharpness
+    std::vector<int32_t> kv;   // corner vertices ("t corner"), when tags are read
+    std::vector<float> ks;     // their sharpness
     int err_line = 0;          // nonzero: 1-based line (within the chunk) of a malformed face or tag
     int64_t lines = 0;
 };
@@ -61,7 +64,7 @@ inline bool is_f(const char* p, const char* le) { return le - p >= 2 && p[0] == 
 inline bool is_t(const char* p, const char* le) { return le - p >= 2 && p[0] == 't' && (p[1] == ' ' || p[1] == '\t'); }
 
 // One "t" line (after the "t"): appends a crease tag's edges; false if malformed.
-bool parse_tag(const char* q, const char* le, Chunk& c)
+bool parse_tag(const char* q, const char* le, Chunk& c, bool corners)
 {
     std::string line(q, le);
     const char* p = line.c_str();
@@ -82,9 +85,10 @@ bool parse_tag(const char* q, const char* le, Chunk& c)
             ++p;
         }
     }
-    if (type != "crease") return true;
+    const bool corner = corners && type == "corner";
+    if (type != "crease" && !corner) return true;
     const long ni = n[0], nf = n[1];
-    if (ni < 2 || (nf != 1 && nf != ni - 1)) return false;
+    if (corner ? (ni < 1 || (nf != 1 && nf != ni)) : (ni < 2 || (nf != 1 && nf != ni - 1))) return false;
     std::vector<long> v((size_t)ni);
     for (long k = 0; k < ni; ++k) {
         p = skip_ws(p, e);
@@ -98,6 +102,13 @@ bool parse_tag(const char* q, const char* le, Chunk& c)
         f[(size_t)k] = std::strtof(p, &end);
         if (end == p) return false;
         p = end;
+    }
+    if (corner) {
+        for (long k = 0; k < ni; ++k) {
+            c.kv.push_back((int32_t)v[(size_t)k]);
+            c.ks.push_back(nf == 1 ? f[0] : f[(size_t)k]);
+        }
+        return true;
     }
     for (long k = 0; k + 1 < ni; ++k) {
         c.cv.push_back((int32_t)v[(size_t)k]);
@@ -117,8 +128,9 @@ void count_pass(Chunk& c)
     }
 }
 
-// base: vertices defined before this chunk; tags: read "t crease" lines
-void parse_pass(Chunk& c, int64_t base, bool tags)
+// base: vertices defined before this chunk; tags: read "t crease" lines;
+// corners: also "t corner" lines
+void parse_pass(Chunk& c, int64_t base, bool tags, bool corners)
 {
     int64_t nv = base;
     std::string tmp;
@@ -157,7 +169,7 @@ void parse_pass(Chunk& c, int64_t base, bool tags)
             if (c.err_line) break;
             c.fo.push_back(order);
         } else if (tags && is_t(s, le)) {
-            if (!parse_tag(s + 1, le, c)) { c.err_line = (int)c.lines; break; }
+            if (!parse_tag(s + 1, le, c, corners)) { c.err_line = (int)c.lines; break; }
         }
         p = le + 1;
     }
@@ -170,11 +182,12 @@ int nthreads_for(size_t bytes)
     return (int)std::max<size_t>(1, std::min<size_t>(hc ? hc : 1, by_size));
 }
 
-int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
+int obj_read(const char* path, slak_mesh* out, slak_creases* cr, slak_corners* ko = nullptr)
 {
     if (!path || !out) return SLAK_ERR_INVALID_ARG;
     std::memset(out, 0, sizeof(*out));
     if (cr) std::memset(cr, 0, sizeof(*cr));
+    if (ko) std::memset(ko, 0, sizeof(*ko));
     FILE* f = std::fopen(path, "rb");
     if (!f) return SLAK_ERR_INVALID_ARG;
     std::fseek(f, 0, SEEK_END);
@@ -210,7 +223,7 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
     run([&](int t) { count_pass(ch[t]); });
     std::vector<int64_t> vbase(nt + 1, 0);
     for (int t = 0; t < nt; ++t) vbase[t + 1] = vbase[t] + ch[t].nv;
-    run([&](int t) { parse_pass(ch[t], vbase[t], cr != nullptr); });
+    run([&](int t) { parse_pass(ch[t], vbase[t], cr != nullptr, ko != nullptr); });
 
     int64_t F = 0, N = 0, V = vbase[nt];
     for (auto& c : ch) {
@@ -252,10 +265,29 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
     });
     ptr[F] = (int32_t)N;
     for (int64_t c = 0; c < N && !bad; ++c) bad = ids[c] >= V;
-    int64_t C = 0;
+    int64_t C = 0, K = 0;
     for (auto& c : ch) {
         C += (int64_t)c.cs.size();
+        K += (int64_t)c.ks.size();
         for (int32_t x : c.cv) bad |= x >= V;
+        for (int32_t x : c.kv) bad |= x >= V;
+    }
+    int32_t* kverts = nullptr;
+    float* ksharp = nullptr;
+    if (!bad && ko && K > 0) {
+        kverts = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t)K));
+        ksharp = static_cast<float*>(std::malloc(sizeof(float) * (size_t)K));
+        if (!kverts || !ksharp) {
+            std::free(kverts); std::free(ksharp);
+            std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
+            return SLAK_ERR_OOM;
+        }
+        int64_t o = 0;
+        for (auto& c : ch) {
+            std::memcpy(kverts + o, c.kv.data(), sizeof(int32_t) * c.kv.size());
+            std::memcpy(ksharp + o, c.ks.data(), sizeof(float) * c.ks.size());
+            o += (int64_t)c.ks.size();
+        }
     }
     int32_t* cverts = nullptr;
     float* csharp = nullptr;
@@ -263,7 +295,7 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
         cverts = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * 2 * (size_t)C));
         csharp = static_cast<float*>(std::malloc(sizeof(float) * (size_t)C));
         if (!cverts || !csharp) {
-            std::free(cverts); std::free(csharp);
+            std::free(cverts); std::free(csharp); std::free(kverts); std::free(ksharp);
             std::free(ptr); std::free(ids); std::free(vals); std::free(verts);
             return SLAK_ERR_OOM;
         }
@@ -283,6 +315,11 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
         cr->verts = cverts;
         cr->sharpness = csharp;
     }
+    if (ko) {
+        ko->count = K;
+        ko->verts = kverts;
+        ko->sharpness = ksharp;
+    }
     out->type = (F > 0 && min_order == 3 && max_order == 3) ? SLAK_MESH_TRI
               : (F > 0 && min_order == 4 && max_order == 4) ? SLAK_MESH_QUAD : SLAK_MESH_POLY;
     out->is_reduced = 1;
@@ -297,10 +334,12 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr)
     return SLAK_OK;
 }
 
-int obj_write(const char* path, const slak_mesh* m, const slak_creases* cr)
+int obj_write(const char* path, const slak_mesh* m, const slak_creases* cr, const slak_corners* ko = nullptr)
 {
     if (cr && cr->count < 0) return SLAK_ERR_INVALID_ARG;
     if (cr && cr->count > 0 && (!cr->verts || !cr->sharpness)) return SLAK_ERR_INVALID_ARG;
+    if (ko && ko->count < 0) return SLAK_ERR_INVALID_ARG;
+    if (ko && ko->count > 0 && (!ko->verts || !ko->sharpness)) return SLAK_ERR_INVALID_ARG;
     if (!path || !m || m->nverts < 0 || m->nfaces < 0 || (m->nverts > 0 && !m->verts)) return SLAK_ERR_INVALID_ARG;
     const int fixed = m->type == SLAK_MESH_QUAD ? 4 : m->type == SLAK_MESH_TRI ? 3 : 0;
     if (m->nfaces > 0 && (!m->ids || (!fixed && !m->ptr))) return SLAK_ERR_INVALID_ARG;
@@ -354,6 +393,13 @@ int obj_write(const char* path, const slak_mesh* m, const slak_creases* cr)
             ok &= std::fwrite(line, 1, (size_t)n, f) == (size_t)n;
         }
     }
+    if (ko) {
+        char line[96];
+        for (int64_t k = 0; k < ko->count && ok; ++k) {
+            const int n = std::snprintf(line, sizeof line, "t corner 1/1/0 %d %.9g\n", ko->verts[k], ko->sharpness[k]);
+            ok &= std::fwrite(line, 1, (size_t)n, f) == (size_t)n;
+        }
+    }
     ok &= std::fclose(f) == 0;
     return ok ? SLAK_OK : SLAK_ERR_INVALID_ARG;
 }
@@ -376,6 +422,27 @@ int slak_obj_write_creased(const char* path, const slak_mesh* m, const slak_crea
 {
     if (!creases) return SLAK_ERR_INVALID_ARG;
     return obj_write(path, m, creases);
+}
+
+int slak_obj_read_sharp(const char* path, slak_mesh* out, slak_creases* creases, slak_corners* corners)
+{
+    if (!creases || !corners) return SLAK_ERR_INVALID_ARG;
+    return obj_read(path, out, creases, corners);
+}
+
+int slak_obj_write_sharp(const char* path, const slak_mesh* m, const slak_creases* creases,
+                         const slak_corners* corners)
+{
+    return obj_write(path, m, creases, corners);
+}
+
+int slak_obj_free_corners(slak_corners* c)
+{
+    if (!c) return SLAK_ERR_INVALID_ARG;
+    std::free(c->verts);
+    std::free(c->sharpness);
+    std::memset(c, 0, sizeof(*c));
+    return SLAK_OK;
 }
 
 int slak_obj_free_creases(slak_creases* c)

@@ -203,6 +203,8 @@ struct slak_plan {
     int crease_levels = 0;           // ceil(largest sharpness), at most the level count
     int* c_pairs = nullptr;
     float* c_sharp = nullptr;
+    float* c_vcs = nullptr;          // corner sharpness of the base vertices (with corners)
+    std::vector<float> h_vcs;        // its host copy, uploaded at creation
     int* c_mark = nullptr;           // level-0 corner -> live crease entry + 1
     unsigned char* c_bnd0 = nullptr; // base vertices on the boundary (open meshes)
     int *c_vcnt = nullptr, *c_vptr = nullptr, *c_inc = nullptr;
@@ -466,7 +468,7 @@ void launch_creases_t(slak_plan* p, int li, Faces<QUAD> fc, Lc& lc)
     for (int t = 0; t < li; ++t) eps.epid[t] = p->c_ep[t];
     const int64_t nv = (int64_t)V0 + m * ((1ll << li) - 1);
     k_crease_verts<QUAD><<<grid_for(nv), kBlock, 0, str>>>(fc, li, V0, m, L.ids, p->c_cc[li], p->c_cs[li],
-                                                           p->c_vcnt, p->c_vptr, p->c_inc, p->c_bnd0, eps, L.verts,
+                                                           p->c_vcnt, p->c_vptr, p->c_inc, p->c_bnd0, eps, p->c_vcs, L.verts,
                                                            L.o_verts);
     lc.after("k_crease_verts");
 }
@@ -713,6 +715,7 @@ void plan_carve(slak_plan* p, Carver& cv)
         p->c_sharp = cv.take<float>(m);
         p->c_mark = cv.take<int>(p->lv[0].N);
         p->c_bnd0 = p->lv[0].B > 0 ? cv.take<unsigned char>(p->lv[0].V) : nullptr;
+        p->c_vcs = p->h_vcs.empty() ? nullptr : cv.take<float>(p->lv[0].V);
         p->c_vcnt = cv.take<int>(p->lv[0].V);
         p->c_vptr = cv.take<int>(p->lv[0].V + 1);
         p->c_inc = cv.take<int>(2 * m);
@@ -962,16 +965,38 @@ int plan_autotune(slak_plan* p, cudaStream_t str)
 // workspace (the plan does not own them).
 // Crease list sizing from a host copy of the sharpness (one sync): the levels
 // with a live crease.
-static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, cudaStream_t str)
+static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, const int32_t* cverts,
+                             const float* csharp, int64_t nc, cudaStream_t str)
 {
-    std::vector<float> h((size_t)m);
-    cudaError_t e = cudaMemcpyAsync(h.data(), sharp, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, str);
+    std::vector<float> h((size_t)m), hc((size_t)nc);
+    std::vector<int32_t> hv((size_t)nc);
+    cudaError_t e = cudaSuccess;
+    if (m) e = cudaMemcpyAsync(h.data(), sharp, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, str);
+    if (nc && e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), csharp, sizeof(float) * (size_t)nc, cudaMemcpyDeviceToHost, str);
+    if (nc && e == cudaSuccess) e = cudaMemcpyAsync(hv.data(), cverts, sizeof(int32_t) * (size_t)nc, cudaMemcpyDeviceToHost, str);
     if (e == cudaSuccess) e = cudaStreamSynchronize(str);
     if (e != cudaSuccess) { g_detail = std::string("crease sharpness: ") + cudaGetErrorString(e); return cuda_status(e); }
     float smax = 0.0f;
     for (float x : h) {
         if (!std::isfinite(x)) { g_detail = "crease sharpness is not finite"; return SLAK_ERR_INVALID_ARG; }
         smax = std::max(smax, x);
+    }
+    if (nc) {                        // corners: a dense sharpness per base vertex, checked here
+        const int64_t V0 = p->lv[0].V;
+        p->h_vcs.assign((size_t)V0, 0.0f);
+        std::vector<char> seen((size_t)V0, 0);
+        for (int64_t i = 0; i < nc; ++i) {
+            const int32_t v = hv[(size_t)i];
+            const float x = hc[(size_t)i];
+            if (!std::isfinite(x)) { g_detail = "corner sharpness is not finite"; return SLAK_ERR_INVALID_ARG; }
+            if (v < 0 || v >= V0 || seen[(size_t)v]) {
+                g_detail = "corner " + std::to_string(i) + ": vertex out of range or named twice";
+                return SLAK_ERR_BAD_MESH;
+            }
+            seen[(size_t)v] = 1;
+            p->h_vcs[(size_t)v] = std::max(x, 0.0f);
+            smax = std::max(smax, x);
+        }
     }
     const int nlev = (int)p->lv.size();
     int cl = smax > 0.0f ? (int)std::ceil((double)smax) : 0;
@@ -984,7 +1009,8 @@ static int plan_crease_setup(slak_plan* p, const float* sharp, int64_t m, cudaSt
 
 static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, int flags, cudaStream_t str,
                             Workspace* ws, slak_plan** out_plan, const int* cpairs = nullptr,
-                            const float* csharp = nullptr, int64_t ncrease = 0)
+                            const float* csharp = nullptr, int64_t ncrease = 0, const int32_t* kverts = nullptr,
+                            const float* ksharp = nullptr, int64_t ncorner = 0)
 {
     *out_plan = nullptr;
     int rc = validate_mesh(cm, scheme);
@@ -1010,7 +1036,8 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
         for (int k = 0; k < 4 && ce == cudaSuccess; ++k) ce = cudaEventCreateWithFlags(&p->cev[k], cudaEventDisableTiming);
         if (ce != cudaSuccess) rc = cuda_status(ce);
     }
-    if (rc == SLAK_OK && ncrease > 0) rc = plan_crease_setup(p, csharp, ncrease, str);
+    if (rc == SLAK_OK && (ncrease > 0 || ncorner > 0))
+        rc = plan_crease_setup(p, csharp, ncrease, kverts, ksharp, ncorner, str);
     if (rc != SLAK_OK) { free_plan_memory(p); delete p; return rc; }
     Carver dry(nullptr);
     plan_carve(p, dry);
@@ -1034,9 +1061,15 @@ static int plan_create_impl(const slak_mesh* cm, int target_level, int scheme, i
     }
     p->out = o;
     if (ce == cudaSuccess && p->crease_levels > 0) {   // the plan keeps its own copy of the creases
-        ce = cudaMemcpyAsync(p->c_pairs, cpairs, sizeof(int) * 2 * (size_t)ncrease, cudaMemcpyDeviceToDevice, str);
-        if (ce == cudaSuccess)
-            ce = cudaMemcpyAsync(p->c_sharp, csharp, sizeof(float) * (size_t)ncrease, cudaMemcpyDeviceToDevice, str);
+        if (ncrease > 0) {
+            ce = cudaMemcpyAsync(p->c_pairs, cpairs, sizeof(int) * 2 * (size_t)ncrease, cudaMemcpyDeviceToDevice, str);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(p->c_sharp, csharp, sizeof(float) * (size_t)ncrease, cudaMemcpyDeviceToDevice,
+                                     str);
+        }
+        if (ce == cudaSuccess && p->c_vcs)
+            ce = cudaMemcpyAsync(p->c_vcs, p->h_vcs.data(), sizeof(float) * p->h_vcs.size(), cudaMemcpyHostToDevice,
+                                 str);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(str);
     }
     if (ce != cudaSuccess) { free_plan_memory(p); delete p; return cuda_status(ce); }
@@ -1077,31 +1110,51 @@ int slak_plan_create(const slak_mesh* cm, int target_level, int scheme, int flag
                             out_plan);
 }
 
+int slak_plan_create_sharp(const slak_mesh* cm, int target_level, int scheme, int flags,
+                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                           const int32_t* corner_verts, const float* corner_sharpness, int64_t ncorners,
+                           slak_stream_t stream, slak_plan** out_plan)
+{
+    if (!cm || !out_plan || ncreases < 0 || ncorners < 0) return SLAK_ERR_INVALID_ARG;
+    if (ncreases > 0 && (!crease_verts || !crease_sharpness)) return SLAK_ERR_INVALID_ARG;
+    if (ncorners > 0 && (!corner_verts || !corner_sharpness)) return SLAK_ERR_INVALID_ARG;
+    return plan_create_impl(cm, target_level, scheme, flags, reinterpret_cast<cudaStream_t>(stream), nullptr,
+                            out_plan, crease_verts, crease_sharpness, ncreases, corner_verts, corner_sharpness,
+                            ncorners);
+}
+
 int slak_plan_create_creased(const slak_mesh* cm, int target_level, int scheme, int flags,
                              const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
                              slak_stream_t stream, slak_plan** out_plan)
 {
-    if (!cm || !out_plan || ncreases < 0) return SLAK_ERR_INVALID_ARG;
-    if (ncreases > 0 && (!crease_verts || !crease_sharpness)) return SLAK_ERR_INVALID_ARG;
-    return plan_create_impl(cm, target_level, scheme, flags, reinterpret_cast<cudaStream_t>(stream), nullptr,
-                            out_plan, crease_verts, crease_sharpness, ncreases);
+    return slak_plan_create_sharp(cm, target_level, scheme, flags, crease_verts, crease_sharpness, ncreases,
+                                  nullptr, nullptr, 0, stream, out_plan);
 }
 
-int slak_subdivide_creased(const slak_mesh* cm, slak_mesh* rm, int target_level, int scheme,
-                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
-                           slak_stream_t stream)
+int slak_subdivide_sharp(const slak_mesh* cm, slak_mesh* rm, int target_level, int scheme,
+                         const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                         const int32_t* corner_verts, const float* corner_sharpness, int64_t ncorners,
+                         slak_stream_t stream)
 {
     if (!cm || !rm) return SLAK_ERR_INVALID_ARG;
     std::memset(rm, 0, sizeof(*rm));
     slak_plan* p = nullptr;
-    int rc = slak_plan_create_creased(cm, target_level, scheme, 0, crease_verts, crease_sharpness, ncreases, stream,
-                                      &p);
+    int rc = slak_plan_create_sharp(cm, target_level, scheme, 0, crease_verts, crease_sharpness, ncreases,
+                                    corner_verts, corner_sharpness, ncorners, stream, &p);
     if (rc != SLAK_OK) return rc;
     rc = slak_plan_execute(p, stream);
     if (rc == SLAK_OK) rc = slak_plan_status(p, stream);
     if (rc == SLAK_OK) rc = slak_plan_release_output(p, rm);
     slak_plan_destroy(p);
     return rc;
+}
+
+int slak_subdivide_creased(const slak_mesh* cm, slak_mesh* rm, int target_level, int scheme,
+                           const int32_t* crease_verts, const float* crease_sharpness, int64_t ncreases,
+                           slak_stream_t stream)
+{
+    return slak_subdivide_sharp(cm, rm, target_level, scheme, crease_verts, crease_sharpness, ncreases, nullptr,
+                                nullptr, 0, stream);
 }
 
 int slak_plan_execute(slak_plan* p, slak_stream_t stream)

@@ -5,8 +5,8 @@
 The mesh is read on the host (multi-threaded parse), refined by slak_subdivide
 (the drop-in call, host buffers copied in and out) and written with exact
 float32 positions, for visual checks of the refinement.  A file with
-"t crease" tags is refined with those creases (slak_plan_create_creased), unless
---no-creases is given.
+"t crease" / "t corner" tags is refined with that sharpness
+(slak_plan_create_sharp), unless --no-creases is given.
 """
 from __future__ import annotations
 
@@ -21,23 +21,24 @@ def main(argv=None):
     ap.add_argument("output")
     ap.add_argument("--levels", type=int, default=2)
     ap.add_argument("--scheme", default="slak", choices=["slak", "lak"])
-    ap.add_argument("--no-creases", action="store_true", help="ignore the file's crease tags")
+    ap.add_argument("--no-creases", action="store_true", help="ignore the file's crease and corner tags")
     a = ap.parse_args(argv)
     from . import api, meshio
     from .mesh import LAK, SLAK
     t0 = time.perf_counter()
-    mesh, creases = meshio.read_obj_creased(a.input)
+    mesh, creases, corners = meshio.read_obj_sharp(a.input)
     scheme = SLAK if a.scheme == "slak" else LAK
     ncr = 0 if a.no_creases else int(creases[1].size)
-    if ncr:
-        out = api.subdivide(mesh, a.levels, scheme, creases=creases)
+    nco = 0 if a.no_creases else int(corners[1].size)
+    if ncr or nco:
+        out = api.subdivide(mesh, a.levels, scheme, creases=creases, corners=corners)
     else:
         cls = api.CatmullClark if scheme == SLAK else api.LAKCatmullClark
         rm = api.DeviceMesh()
         cls.subdivideIteratively(api.DeviceMesh.from_host(mesh), rm, a.levels)
         out = rm.to_host()
     meshio.write_obj(a.output, out)
-    print(f"{a.input}: {mesh.nfaces} faces, {mesh.nverts} verts, {ncr} crease edges -> {out.nfaces} quads, "
+    print(f"{a.input}: {mesh.nfaces} faces, {mesh.nverts} verts, {ncr} crease edges, {nco} corners -> {out.nfaces} quads, "
           f"{out.nverts} verts ({a.scheme.upper()}, {a.levels} levels) in {time.perf_counter() - t0:.2f} s")
     return 0
 

@@ -109,3 +109,37 @@ def test_invalid_pairs_rejected():
         oc.subdivide_creased(m, 1, SLAK, [[4, 6], [6, 4]], [1.0, 2.0])   # named twice
     with pytest.raises(ValueError):
         oc.subdivide_creased(m, 1, SLAK, [[0, 8]], [1.0])        # out of range
+
+
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+def test_corner_tags_pin_vertices(scheme):
+    """Vertex sharpness ("t corner" tags): a corner of sharpness >= the level
+    count never moves; sharpness 0.5 blends the first level's smooth point
+    half-way to the original; a corner on a crease vertex wins the rule."""
+    m = _lak(cube(), scheme)
+    V = np.asarray(m.verts, np.float32)
+    none = np.zeros((0, 2), np.int32), np.zeros(0, np.float32)
+    r = oc.subdivide_creased(m, 3, scheme, *none, corners=(np.arange(8), np.full(8, 5.0, np.float32)))
+    assert np.array_equal(r.verts[:8], V[:8])
+    smooth = oracle.subdivide(m, 3, scheme)
+    assert not np.array_equal(smooth.verts[:8], V[:8])
+    half = oc.subdivide_creased(m, 1, scheme, *none, corners=([2], [0.5]))
+    s1 = oracle.subdivide(m, 1, scheme).verts
+    assert np.allclose(half.verts[2], 0.5 * s1[2] + 0.5 * V[2], atol=1e-6)
+    changed = np.flatnonzero((half.verts != s1).any(1))
+    assert changed.tolist() == [2]
+    # sharpness 1 is spent after one level: level 2 moves the vertex again
+    r2 = oc.subdivide_creased(m, 2, scheme, *none, corners=([2], [1.0]))
+    assert not np.array_equal(r2.verts[2], V[2])
+    # a crease through vertex 4 (crease rule) plus a corner tag on it: corner wins
+    both = oc.subdivide_creased(m, 1, scheme, [[4, 6], [4, 5]], [3.0, 3.0], corners=([4], [2.0]))
+    assert np.array_equal(both.verts[4], V[4])
+
+
+def test_invalid_corners_rejected():
+    m = cube()
+    none = np.zeros((0, 2), np.int32), np.zeros(0, np.float32)
+    with pytest.raises(ValueError):
+        oc.subdivide_creased(m, 1, SLAK, *none, corners=([8], [1.0]))           # out of range
+    with pytest.raises(ValueError):
+        oc.subdivide_creased(m, 1, SLAK, *none, corners=([3, 3], [1.0, 2.0]))   # named twice

@@ -131,3 +131,44 @@ def test_invalid_creases_rejected(pairs, sharp, code):
     with pytest.raises(_abi.SlakError) as ei:
         api.subdivide(m, 2, SLAK, creases=(np.array(pairs, np.int32), np.array(sharp, np.float32)))
     assert ei.value.code == code
+
+
+def _same_sharp(mesh, levels, scheme, pairs, sharp, corners, flags=0):
+    ref = oc.subdivide_creased(mesh, levels, scheme, pairs, sharp, corners=corners)
+    got = api.subdivide(mesh, levels, scheme, flags, creases=(pairs, sharp), corners=corners)
+    assert np.array_equal(got.ids, ref.ids)
+    assert np.array_equal(_bits(got.verts), _bits(ref.verts))
+    return got
+
+
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+def test_corners_bit_exact(scheme):
+    """Corner tags alone, with creases, fractional, on crease vertices and on
+    boundary vertices: bit for bit against the restatement, on the fast path,
+    the general path and a graph replay."""
+    rng = np.random.default_rng(7)
+    none = (np.zeros((0, 2), np.int32), np.zeros(0, np.float32))
+    cube_m = _lak(cube(), scheme)
+    _same_sharp(cube_m, 4, scheme, *none, (np.arange(8, dtype=np.int32), np.full(8, 10.0, np.float32)))
+    _same_sharp(cube_m, 3, scheme, *none, (np.array([1, 6], np.int32), np.array([0.5, 1.5], np.float32)))
+    for make, levels in ((lambda: meshgen.mixed_torus(40, 32, 0.05, 0.03, 0.005, seed=4), 4),
+                         (lambda: open_mixed(), 3)):
+        m = _lak(make(), scheme)
+        pairs, sharp = _random_creases(m, 0.15, 1)
+        kv = np.unique(np.concatenate([pairs[:40, 0], rng.integers(0, m.nverts, 60)])).astype(np.int32)
+        ks = rng.choice(np.array([0.25, 0.5, 1.0, 2.5, 6.0], np.float32), kv.size)
+        a = _same_sharp(m, levels, scheme, pairs, sharp, (kv, ks))
+        g = api.subdivide(m, levels, scheme, _abi.PLAN_GENERAL, creases=(pairs, sharp), corners=(kv, ks))
+        assert np.array_equal(_bits(g.verts), _bits(a.verts))
+        _same_sharp(m, levels, scheme, *none, (kv, ks))            # corners without creases
+
+
+@pytest.mark.parametrize("kv,ks,code", [
+    ([8], [1.0], _abi.SLAK_ERR_BAD_MESH),                  # out of range
+    ([3, 3], [1.0, 2.0], _abi.SLAK_ERR_BAD_MESH),          # named twice
+    ([3], [float("inf")], _abi.SLAK_ERR_INVALID_ARG),      # not finite
+])
+def test_invalid_corners_rejected(kv, ks, code):
+    with pytest.raises(_abi.SlakError) as ei:
+        api.subdivide(cube(), 2, SLAK, corners=(np.array(kv, np.int32), np.array(ks, np.float32)))
+    assert ei.value.code == code

@@ -26,8 +26,8 @@ def test_obj_subdivide_round_trip(tmp_path, scheme):
 
 @pytest.mark.parametrize("scheme", ["slak", "lak"])
 def test_obj_crease_tags_subdivide(tmp_path, scheme):
-    """A file with "t crease" tags is refined with its creases: the result
-    reads back as the crease restatement's refined mesh."""
+    """A file with "t crease" and "t corner" tags is refined with them: the
+    result reads back as the restatement's refined mesh."""
     from oracle import creases as oc
     src = meshgen.mixed_torus(24, 20, 0.05, 0.03, 0.005, seed=9)
     ids = np.asarray(src.ids)
@@ -38,11 +38,13 @@ def test_obj_crease_tags_subdivide(tmp_path, scheme):
     pairs = np.stack([ids[pick], ids[pick + 1]], 1).astype(np.int32)       # each face's first edge
     pairs = np.unique(np.sort(pairs, 1), axis=0)
     sharp = rng.choice(np.array([0.5, 1.0, 2.5, 4.0], np.float32), pairs.shape[0])
+    kv = np.unique(rng.integers(0, src.nverts, 30)).astype(np.int32)
+    ks = rng.choice(np.array([0.5, 1.0, 3.0], np.float32), kv.size)
     inp, out = tmp_path / "in.obj", tmp_path / "out.obj"
-    meshio.write_obj(str(inp), src, creases=(pairs, sharp))
+    meshio.write_obj(str(inp), src, creases=(pairs, sharp), corners=(kv, ks))
     assert objsubdiv.main([str(inp), str(out), "--levels", "3", "--scheme", scheme]) == 0
     got = meshio.read_obj(str(out))
-    mesh, cr = meshio.read_obj_creased(str(inp))
-    ref = oc.subdivide_creased(mesh, 3, SLAK if scheme == "slak" else LAK, *cr)
+    mesh, cr, ko = meshio.read_obj_sharp(str(inp))
+    ref = oc.subdivide_creased(mesh, 3, SLAK if scheme == "slak" else LAK, *cr, corners=ko)
     assert np.array_equal(got.ids, ref.ids)
     assert np.array_equal(got.verts[:, :3].view(np.uint32), ref.verts[:, :3].view(np.uint32))

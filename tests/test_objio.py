@@ -174,3 +174,34 @@ def test_malformed_crease_tags_rejected(tmp_path, bad):
     with pytest.raises(_abi.SlakError):
         meshio.read_obj_creased(str(path))
     meshio.read_obj(str(path))           # the plain reader skips tags
+
+
+def test_corner_tags(tmp_path):
+    path = tmp_path / "k.obj"
+    path.write_text(CREASED + "t corner 2/1/0 3 4 7.5\nt corner 1/1/0 0 0.25\nt corner 2/2/0 1 2 1 2\n")
+    m, (pairs, sharp), (kv, ks) = meshio.read_obj_sharp(str(path))
+    assert pairs.shape == (5, 2)
+    # CREASED's own "t corner 1/1/0 4 10" first (the plan, not the reader, rejects a vertex named twice)
+    assert kv.tolist() == [4, 3, 4, 0, 1, 2] and ks.tolist() == [10.0, 7.5, 7.5, 0.25, 1.0, 2.0]
+    # the crease-only reader skips corner tags, even malformed ones
+    bad = tmp_path / "kb.obj"
+    bad.write_text(CREASED + "t corner 2/5/0 3 4 1\n")
+    assert meshio.read_obj_creased(str(bad))[1][1].size == 5
+    with pytest.raises(_abi.SlakError):
+        meshio.read_obj_sharp(str(bad))
+    oor = tmp_path / "ko.obj"
+    oor.write_text(CREASED + "t corner 1/1/0 9 1\n")          # vertex out of range
+    with pytest.raises(_abi.SlakError):
+        meshio.read_obj_sharp(str(oor))
+
+
+def test_corner_tags_round_trip(tmp_path):
+    m = meshgen.torus(8, 6, seed=2)
+    kv = np.array([0, 5, 17], np.int32)
+    ks = np.array([0.5, 3.0, 10.0], np.float32)
+    pairs = np.array([[0, 1]], np.int32)
+    path = tmp_path / "r.obj"
+    meshio.write_obj(str(path), m, creases=(pairs, np.array([2.0], np.float32)), corners=(kv, ks))
+    r, (p2, s2), (k2, w2) = meshio.read_obj_sharp(str(path))
+    assert np.array_equal(r.ids, m.ids) and np.array_equal(p2, pairs)
+    assert np.array_equal(k2, kv) and np.array_equal(w2.view(np.uint32), ks.view(np.uint32))
