@@ -510,7 +510,25 @@ def run_batch(args, torch, dist, rank, ws):
            "plain": "slak_subdivide per mesh (allocates and frees its output per call)",
            "plan_loop": "per mesh: plan created untimed, one eager execution timed with CUDA events",
            "batched": "slak_batch, one CUDA graph per execution"}
-    b.close()
+    b.close()                                            # its outputs go before the one-call form's arrive
+
+    # the one-call form (slak_subdivide_batched): creation, per-mesh output
+    # allocations and one eager execution, wall clock like the plain loop's bracket
+    n = len(cins)
+    arr = (_abi.SlakMesh * n)(*cins)
+    lvs = (ctypes.c_int * n)(*[l for _, l in items])
+    res = (_abi.SlakMesh * n)()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _abi.check(lib.slak_subdivide_batched(arr, lvs, n, scheme, res, sh), "slak_subdivide_batched")
+    torch.cuda.synchronize()
+    one_ms = _max_over_ranks(dist, (time.perf_counter() - t0) * 1e3)
+    for i in range(n):
+        lib.slak_mesh_free(ctypes.byref(res[i]))     # elements share the array's memory
+    out.update({"one_call_ms": one_ms, "one_call_value": faces * ws / (one_ms * 1e-3),
+                "speedup_one_call_vs_plain": plain_ms / one_ms,
+                "one_call": "slak_subdivide_batched: batch creation, per-mesh cudaMalloc of the outputs, one eager "
+                            "execution (wall clock)"})
     return out
 
 
