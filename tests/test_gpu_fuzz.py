@@ -83,3 +83,39 @@ def test_random_meshes_bit_exact(seed, scheme):
     assert np.array_equal(_bits(got.verts), _bits(ref.verts))
     gen = api.subdivide(mesh, levels, scheme, api._abi.PLAN_GENERAL)
     assert np.array_equal(gen.ids, got.ids) and np.array_equal(_bits(gen.verts), _bits(got.verts))
+
+
+def _random_sharp(mesh, seed):
+    """A random share of the edges tagged with random sharpness (whole and
+    fractional, some above the level count) and a few random corners."""
+    from oracle import creases as oc
+    rng = np.random.default_rng(1000 + seed)
+    ptr = mesh.ptr if mesh.ptr is not None else np.arange(mesh.nfaces + 1) * 4
+    ids = np.asarray(mesh.ids, np.int64)
+    nxt = oc._next_corner(ptr, ids.size, mesh.type == 1)
+    e = np.unique(np.sort(np.stack([ids, ids[nxt]], 1), 1), axis=0)
+    pick = e[rng.random(e.shape[0]) < rng.uniform(0.02, 0.4)]
+    sharp = np.where(rng.random(pick.shape[0]) < 0.5, rng.integers(1, 6, pick.shape[0]),
+                     rng.uniform(0.05, 4.0, pick.shape[0])).astype(np.float32)
+    V = int(np.asarray(mesh.verts).shape[0])
+    kv = rng.choice(V, int(rng.integers(0, min(V, 8) + 1)), replace=False).astype(np.int32)
+    ks = rng.uniform(0.1, 5.0, kv.size).astype(np.float32)
+    return pick.astype(np.int32), sharp, (kv, ks)
+
+
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+@pytest.mark.parametrize("seed", list(range(20)))
+def test_random_creases_bit_exact(seed, scheme):
+    from oracle import creases as oc
+    mesh, levels = _random_case(seed)
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    if scheme == SLAK and not _bowtie_free(mesh):
+        pytest.skip("a bowtie boundary vertex (SLAK differs there by design)")
+    pairs, sharp, corners = _random_sharp(mesh, seed)
+    ref = oc.subdivide_creased(mesh, levels, scheme, pairs, sharp, corners=corners)
+    got = api.subdivide(mesh, levels, scheme, creases=(pairs, sharp), corners=corners)
+    assert np.array_equal(got.ids, ref.ids)
+    assert np.array_equal(_bits(got.verts), _bits(ref.verts))
+    gen = api.subdivide(mesh, levels, scheme, api._abi.PLAN_GENERAL, creases=(pairs, sharp), corners=corners)
+    assert np.array_equal(gen.ids, got.ids) and np.array_equal(_bits(gen.verts), _bits(got.verts))
