@@ -306,3 +306,64 @@ def test_degenerate_faces_rejected(scheme, flags):
         with pytest.raises(api._abi.SlakError) as e:
             api.subdivide(bad, 2, scheme, flags)
         assert e.value.code == api._abi.SLAK_ERR_BAD_MESH
+
+
+def _with_unused_vertices(mesh):
+    """The mesh with three vertices no face uses: one before all others (ids
+    shift by one), one in the middle and one at the end."""
+    from slak_b200.mesh import from_arrays
+    V = np.asarray(mesh.verts, np.float32)[:, :3]
+    mid = V.shape[0] // 2
+    ids = np.asarray(mesh.ids, np.int64)
+    ids = ids + 1 + (ids >= mid)
+    far = np.array([[7.0, -3.0, 2.0]], np.float32)
+    V2 = np.concatenate([far, V[:mid], far * 2, V[mid:], far * 3])
+    ptr = mesh.ptr if mesh.ptr is not None else np.arange(mesh.nfaces + 1) * 4
+    return from_arrays(np.asarray(ptr), ids.astype(np.int32), V2)
+
+
+UNUSED = [("torus", lambda: meshgen.torus(12, 10), 3),
+          ("mixed", lambda: meshgen.mixed_torus(16, 12, 0.08, 0.05, 0.005, seed=9), 3),
+          ("grid", lambda: open_grid(10, 7), 3)]
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("name,make,levels", UNUSED, ids=[c[0] for c in UNUSED])
+def test_unused_vertices(name, make, levels, scheme):
+    """A vertex that no face uses has valence 0: the reference's vertex rule
+    divides 0 by 0 there (vertexSum CatmullClarkKernels.cuh:634-652; LAK
+    LAKCatmullClarkImpl.cu:200-221), so its refined position is NaN and
+    nothing else changes.  Same on the fast and general paths, plain and
+    compensated; ids exact, positions bit-exact with NaN == NaN."""
+    mesh = make()
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    m = _with_unused_vertices(mesh)
+    got, ref = _check(m, levels, scheme)
+    assert _bits_equal(got.verts, ref.verts)
+    nan_rows = np.flatnonzero(np.isnan(got.verts[:, :3]).any(1))
+    V0 = mesh.nverts
+    assert np.array_equal(nan_rows, [0, V0 // 2 + 1, V0 + 2])
+    base = api.subdivide(mesh, levels, scheme)
+    assert got.nfaces == base.nfaces and got.nverts == base.nverts + 3
+    for flags in (api._abi.PLAN_GENERAL, api._abi.PLAN_COMPENSATED,
+                  api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL):
+        o = api.subdivide(m, levels, scheme, flags)
+        assert np.array_equal(o.ids, got.ids)
+        assert np.array_equal(np.flatnonzero(np.isnan(o.verts[:, :3]).any(1)), nan_rows)
+    a = api.subdivide(m, levels, scheme, api._abi.PLAN_COMPENSATED)
+    b = api.subdivide(m, levels, scheme, api._abi.PLAN_COMPENSATED | api._abi.PLAN_GENERAL)
+    assert _bits_equal(a.verts, b.verts)
+
+
+@pytest.mark.parametrize("cls", [api.CatmullClark, api.LAKCatmullClark])
+def test_empty_mesh(cls):
+    """No faces (any face type): nothing to refine, the call succeeds and the
+    output mesh is left untouched, as for a QUAD input at level 0."""
+    from slak_b200.mesh import Mesh
+    for t in (0, 1, 2):
+        m = Mesh(t, np.zeros(0, np.int32), np.zeros((0, 4), np.float32),
+                 None if t == 1 else np.zeros(1, np.int32), None, 0, 4 if t == 1 else 0, True)
+        rm = api.DeviceMesh()
+        cls.subdivideIteratively(api.DeviceMesh.from_host(m), rm, 2)
+        assert rm.ids is None and rm.nfaces == 0
