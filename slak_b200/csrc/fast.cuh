@@ -270,6 +270,22 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     const int eidp_x = Q.y - VF1, eidp_px = Q.w - VF1;   // P's edge ids of x and prev(x)
     int br_x = 0, br_px = 0;                             // their boundary ranks
     if (BND && valid) { br_x = __ldg(p.brank + eidp_x); br_px = __ldg(p.brank + eidp_px); }
+    // quad P: the lane of the min->max half-edge of P's edge through x owns
+    // its edge work (below), which gathers three positions of the twin side,
+    // two of them behind ids.  The ids depend on Q and tw1x alone; at the last
+    // level (no state to write, registers to spare) they are fetched now,
+    // beside the quad's own gathers, and the edge work waits for one round
+    // trip instead of two.
+    bool own = false;
+    int ei2 = 0, eo3 = 0;
+    if constexpr (PQ && !STATE) {
+        const int un = __shfl_sync(0xffffffffu, Q.x, ln);     // every lane takes part
+        own = valid && (!BND || tw1x >= 0) && Q.x < un;
+        if (own) {
+            ei2 = __ldg(ids + 4 * (int64_t)tw1x + 3);
+            eo3 = __ldg(ids + 4 * (int64_t)qnext(tw1x) + 1);
+        }
+    }
 
     // face point of quad x
     float4 fp;
@@ -320,6 +336,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
             if (j < 4 * nq) __stcs(dst + j, sq[(j & 3) * SQ + (j >> 2)]);
         }
     }
+
     if (valid) {
         st4(R, (int64_t)d.V + x, fp);
         // records of corner x for its vertex's pass (full 32-byte sectors at slot s1)
@@ -405,11 +422,10 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
         const float4 Pu = shfl4(c0, ln), Fnh = shfl4(fp, ln);
         if (BND && valid && tw1x < 0) {        // the only half-edge of a boundary edge owns it
             boundary_edge<LAK, STATE>(d, c, R, Q.x, u, Q.y, br_x, c0, Pu, c1, c2, fp, Fnh);
-        } else if (valid && Q.x < u) {
+        } else if (STATE ? valid && Q.x < u : own) {
             const int h2 = tw1x, nh2 = qnext(h2), fh2 = d.V1 + (h2 >> 2);
-            const float4 Pf2 = ldg4(P, fh2);
-            const int ei2 = __ldg(ids + 4 * (int64_t)h2 + 3), eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1);
-            const float4 Pi2 = ldg4(P, ei2), Po3 = ldg4(P, eo3);
+            if (STATE) { ei2 = __ldg(ids + 4 * (int64_t)h2 + 3); eo3 = __ldg(ids + 4 * (int64_t)nh2 + 1); }
+            const float4 Pf2 = ldg4(P, fh2), Pi2 = ldg4(P, ei2), Po3 = ldg4(P, eo3);
             float4 Fh2, Fnh2;
             if (!LAK) {
                 Fh2 = f4_mul(f4_add(f4_add(Pu, Pf2), f4_add(c1, Pi2)), 0.25f);
