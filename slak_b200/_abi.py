@@ -18,6 +18,9 @@ STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: 
 
 PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE = 1, 2, 4, 8, 16
 
+# SLAK_B200_ABI_VERSION of include/slak_b200.h, which the structs and signatures here follow
+ABI_VERSION = 1
+
 # every symbol include/slak_b200.h declares
 EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "slak_subdivide", "slak_mesh_free",
            "slak_workspace_release", "slak_subdivide_level_noalloc", "slak_obj_read", "slak_obj_write",
@@ -150,6 +153,9 @@ def lib():
                   "slak_plan_output", "slak_plan_release_output", "slak_plan_num_levels",
                   "slak_plan_level_stats", "slak_plan_destroy"):
             getattr(L, n).restype = I
+        if L.slak_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{_paths.LIB_SLAK} has ABI version {L.slak_abi_version()}, these bindings "
+                               f"expect {ABI_VERSION}: rebuild it with __graft_entry__.build()")
         _lib = L
     return _lib
 

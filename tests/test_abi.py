@@ -30,7 +30,9 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_version_and_status_strings(lib):
-    assert lib.slak_abi_version() == 1
+    hdr = open(os.path.join(_paths.INCLUDE_DIR, "slak_b200.h")).read()
+    declared = int(re.search(r"#define SLAK_B200_ABI_VERSION (\d+)", hdr).group(1))
+    assert lib.slak_abi_version() == declared == _abi.ABI_VERSION
     for code in range(0, 8):
         s = _abi.status_string(code)
         assert s and s != "unknown status"
