@@ -367,3 +367,20 @@ def test_empty_mesh(cls):
         rm = api.DeviceMesh()
         cls.subdivideIteratively(api.DeviceMesh.from_host(m), rm, 2)
         assert rm.ids is None and rm.nfaces == 0
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+def test_too_large_rejected(scheme):
+    """Indices are 32-bit: a level whose refined mesh would reach 2^31
+    corners or vertices is refused with SLAK_ERR_UNSUPPORTED when the plan is
+    sized, before any level runs or any output is allocated.  The 32x32 torus
+    (4,096 corners) passes 2^31 refined corners at its tenth level."""
+    m = meshgen.torus(32, 32)
+    if scheme == LAK:
+        m = m.with_quad_ptr()
+    for levels in (10, 14):
+        with pytest.raises(api._abi.SlakError) as e:
+            api.subdivide(m, levels, scheme)
+        assert e.value.code == api._abi.SLAK_ERR_UNSUPPORTED
+    got, ref = _check(m, 3, scheme)                 # the library is still usable
+    assert _bits_equal(got.verts, ref.verts)
