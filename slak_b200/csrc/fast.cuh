@@ -65,6 +65,16 @@ __device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
                        __shfl_xor_sync(0xffffffffu, v.z, m), __shfl_xor_sync(0xffffffffu, v.w, m));
 }
 
+// A refined position.  At the last level (no STATE) no kernel on the device
+// reads it again, so it is stored streaming and leaves L2 to the slot records
+// k_g3 reads back.
+template <bool STATE>
+__device__ __forceinline__ void st_pos(float* R, int64_t i, float4 v)
+{
+    if constexpr (STATE) st4(R, i, v);
+    else st4_cs(R, i, v);
+}
+
 // rank of corner `a` among the four corners of an edge point
 __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a) + (c < a) + (d < a); }
 
@@ -338,7 +348,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     }
 
     if (valid) {
-        st4(R, (int64_t)d.V + x, fp);
+        st_pos<STATE>(R, (int64_t)d.V + x, fp);
         // records of corner x for its vertex's pass (full 32-byte sectors at slot s1)
         z.Z[2 * (int64_t)s1] = fp;
         z.Z[2 * (int64_t)s1 + 1] = LAK ? c3 : c1;
@@ -394,7 +404,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
                 }
                 yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(c2, 2.0f)), 4.0f);
             }
-            st4(R, (int64_t)d.V1 + (x >> 2), yv);
+            st_pos<STATE>(R, (int64_t)d.V1 + (x >> 2), yv);
         }
 
         // SLAK edge point N1 + x: half-edges 4x+2 (tail f, quad x) and 4 prev(x)+1 (tail e_in(x), quad prev x)
@@ -747,7 +757,7 @@ __device__ __forceinline__ void g3_vertex(FastDims d, const float* __restrict__ 
             yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
         }
         if (BND && (fl[0] | fl[1] | fl[2] | fl[3])) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
-        st4(R, v, yv);
+        st_pos<STATE>(R, v, yv);
         if (STATE) c.sptr[v] = b;
         return;
     }
@@ -805,7 +815,7 @@ __device__ __forceinline__ void g3_vertex(FastDims d, const float* __restrict__ 
         else yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
     }
     if (BND) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
-    st4(R, v, yv);
+    st_pos<STATE>(R, v, yv);
     if (STATE) c.sptr[v] = b;
 }
 
@@ -883,7 +893,7 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
     }
     if (lane == 0) {
         if (BND) yv = boundary_vertex<LAK>(P, z, b, b + n, Pv, yv);
-        st4(R, v, yv);
+        st_pos<STATE>(R, v, yv);
         if (STATE) c.sptr[v] = b;
     }
 }
