@@ -75,6 +75,17 @@ __device__ __forceinline__ void st_pos(float* R, int64_t i, float4 v)
     else st4_cs(R, i, v);
 }
 
+// The slot records k_g1 writes and k_g3 reads back once.  They are stored
+// with an L2 evict-last policy, so the share of them that L2 can hold (most
+// of them below the last level) is still there when k_g3 streams them.
+__device__ __forceinline__ void st4_keep(float4* p, float4 v)
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
+                 :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol));
+}
+
 // rank of corner `a` among the four corners of an edge point
 __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a) + (c < a) + (d < a); }
 
@@ -350,8 +361,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
     if (valid) {
         st_pos<STATE>(R, (int64_t)d.V + x, fp);
         // records of corner x for its vertex's pass (full 32-byte sectors at slot s1)
-        z.Z[2 * (int64_t)s1] = fp;
-        z.Z[2 * (int64_t)s1 + 1] = LAK ? c3 : c1;
+        st4_keep(z.Z + 2 * (int64_t)s1, fp);
+        st4_keep(z.Z + 2 * (int64_t)s1 + 1, LAK ? c3 : c1);
         if (LAK) z.T[s1] = Q.w;
         else if (!BND || t1x >= 0) z.rot[t1x] = s1;
         if (BND && !LAK && tw1x < 0) z.rot[s1] = s1;      // no rotation across the boundary: a safe index
