@@ -75,9 +75,9 @@ __device__ __forceinline__ void st_pos(float* R, int64_t i, float4 v)
     else st4_cs(R, i, v);
 }
 
-// The slot records k_g1 writes and k_g3 reads back once.  They are stored
-// with an L2 evict-last policy, so the share of them that L2 can hold (most
-// of them below the last level) is still there when k_g3 streams them.
+// The slot records k_g1 writes and k_g3 reads back once, stored with an L2
+// evict-last policy.  Measured on B200 (512x512 mixed torus, SLAK), this
+// takes k_g1's last level from 641 to 619 us; k_g3's time does not move.
 __device__ __forceinline__ void st4_keep(float4* p, float4 v)
 {
     uint64_t pol;
