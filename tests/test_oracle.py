@@ -196,3 +196,37 @@ def test_boundary_rules_open_grid():
         exp = 0.75 * P[0] + 0.125 * P[1] + 0.125 * P[3]
         assert np.allclose(r.verts64[0], exp)
         assert np.allclose(r.verts[0], exp, atol=1e-6)
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+def test_unused_vertices_oracle(scheme):
+    """Vertices no face uses (valence 0): at level 1 their refined positions
+    are NaN (0/0 in the vertex rule) and every other output row equals the
+    plain mesh's, with the old-vertex ids shifted past the inserted rows."""
+    from slak_b200 import meshgen
+    from slak_b200.mesh import from_arrays
+    base = meshgen.mixed_torus(10, 8, 0.1, 0.05, 0.005, seed=7)
+    V0 = base.nverts
+    mid = V0 // 2
+    P = np.asarray(base.verts, np.float32)[:, :3]
+    ids = np.asarray(base.ids, np.int64)
+    shift = lambda a: a + 1 + (a >= mid)                       # new id of an old vertex
+    far = np.array([[3.0, 1.0, -2.0]], np.float32)
+    m = from_arrays(np.asarray(base.ptr), shift(ids).astype(np.int32),
+                    np.concatenate([far, P[:mid], far, P[mid:], far]))
+    r0 = oracle.subdivide(base, 1, scheme)
+    r1 = oracle.subdivide(m, 1, scheme)
+    assert r1.nverts == r0.nverts + 3 and r1.nfaces == r0.nfaces
+    old = np.arange(V0)
+    v1 = np.asarray(r1.verts)
+    v0 = np.asarray(r0.verts)
+    nan_rows = np.flatnonzero(np.isnan(v1[:, :3]).any(1))
+    assert np.array_equal(nan_rows, [0, mid + 1, V0 + 2])
+    keep = v1[shift(old)]
+    assert np.array_equal(keep.view(np.uint32), v0[:V0].view(np.uint32))
+    assert np.array_equal(v1[V0 + 3:].view(np.uint32), v0[V0:].view(np.uint32))
+    # refined quads: old-vertex ids shifted, face / edge point ids moved by 3
+    q0 = np.asarray(r0.ids, np.int64)
+    q1 = np.asarray(r1.ids, np.int64)
+    expect = np.where(q0 < V0, shift(q0), q0 + 3)
+    assert np.array_equal(q1, expect)
