@@ -89,6 +89,7 @@ bool parse_tag(const char* q, const char* le, Chunk& c, bool corners)
     if (type != "crease" && !corner) return true;
     const long ni = n[0], nf = n[1];
     if (corner ? (ni < 1 || (nf != 1 && nf != ni)) : (ni < 2 || (nf != 1 && nf != ni - 1))) return false;
+    if (ni > e - p || nf > e - p) return false;     // every value takes a character of the line at least
     std::vector<long> v((size_t)ni);
     for (long k = 0; k < ni; ++k) {
         p = skip_ws(p, e);
@@ -160,7 +161,7 @@ void parse_pass(Chunk& c, int64_t base, bool tags, bool corners)
                 long vi = std::strtol(q, &end, 10);
                 if (end == q) { c.err_line = (int)c.lines; break; }
                 const int64_t idx = vi < 0 ? nv + vi : (int64_t)vi - 1;
-                if (vi == 0 || idx < 0) { c.err_line = (int)c.lines; break; }
+                if (vi == 0 || idx < 0 || idx > INT32_MAX) { c.err_line = (int)c.lines; break; }
                 c.fi.push_back((int32_t)idx);
                 ++order;
                 q = end;
@@ -264,13 +265,13 @@ int obj_read(const char* path, slak_mesh* out, slak_creases* cr, slak_corners* k
         }
     });
     ptr[F] = (int32_t)N;
-    for (int64_t c = 0; c < N && !bad; ++c) bad = ids[c] >= V;
+    for (int64_t c = 0; c < N && !bad; ++c) bad = ids[c] < 0 || ids[c] >= V;
     int64_t C = 0, K = 0;
     for (auto& c : ch) {
         C += (int64_t)c.cs.size();
         K += (int64_t)c.ks.size();
-        for (int32_t x : c.cv) bad |= x >= V;
-        for (int32_t x : c.kv) bad |= x >= V;
+        for (int32_t x : c.cv) bad |= x < 0 || x >= V;
+        for (int32_t x : c.kv) bad |= x < 0 || x >= V;
     }
     int32_t* kverts = nullptr;
     float* ksharp = nullptr;
