@@ -29,6 +29,26 @@ class Mesh:
     max_face_order: int = 0
     is_reduced: bool = True
 
+    def __post_init__(self):
+        # the C ABI reads int32 indices and float32 x 4 positions: arrays of
+        # other types are converted here, never reinterpreted
+        def i32(a, name):
+            if a is None:
+                return None
+            a = np.asarray(a)
+            if a.dtype != np.int32:
+                if a.size and (a.min() < np.iinfo(np.int32).min or a.max() > np.iinfo(np.int32).max):
+                    raise ValueError(f"{name}: values do not fit 32-bit indices")
+                a = a.astype(np.int32)
+            return np.ascontiguousarray(a)
+        self.ids = i32(self.ids, "ids")
+        self.ptr = i32(self.ptr, "ptr")
+        self.vals = i32(self.vals, "vals")
+        v = np.asarray(self.verts)
+        if v.ndim != 2 or v.shape[1] != 4:
+            raise ValueError(f"verts: expected shape (V, 4), got {v.shape}")
+        self.verts = np.ascontiguousarray(v, dtype=np.float32)
+
     @property
     def nnz(self) -> int:
         return int(self.ids.shape[0])
