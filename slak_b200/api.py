@@ -73,6 +73,19 @@ class DeviceMesh:
                           t(m.ptr), t(m.ids), t(m.vals), t(m.verts.reshape(-1).astype(np.float32)))
 
     def as_c(self) -> _abi.SlakMesh:
+        import torch                    # dtypes only: the check itself needs no device
+        for name, want, count in (("ptr", torch.int32, self.nfaces + 1), ("ids", torch.int32, self.nnz),
+                                  ("vals", torch.int32, self.nnz), ("verts", torch.float32, 4 * self.nverts)):
+            t = getattr(self, name)
+            if t is None:
+                continue
+            # the C ABI takes the raw pointer: a tensor of another type, layout
+            # or device would be reinterpreted, so it is refused here
+            if t.dtype != want or not t.is_contiguous() or t.device.type != "cuda":
+                raise TypeError(f"DeviceMesh.{name}: expected a contiguous CUDA {want} tensor, "
+                                f"got {t.dtype} on {t.device}")
+            if t.numel() < count:
+                raise ValueError(f"DeviceMesh.{name}: {t.numel()} elements, the counts need {count}")
         c = _abi.SlakMesh()
         c.type, c.is_reduced = int(self.type), int(bool(self.is_reduced))
         c.nfaces, c.nverts, c.nnz, c.max_face_order = self.nfaces, self.nverts, self.nnz, self.max_face_order

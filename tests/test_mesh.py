@@ -34,3 +34,20 @@ def test_verts_shape_checked():
         Mesh(QUAD, np.array([0, 1, 2, 3]), np.zeros((4, 3), np.float32))
     with pytest.raises(ValueError):
         Mesh(QUAD, np.array([0, 1, 2, 3]), np.zeros(16, np.float32))
+
+
+def test_device_mesh_refuses_what_the_abi_would_misread():
+    """DeviceMesh.as_c hands raw pointers to the C ABI, so a tensor of another
+    dtype, a strided view, a host tensor or too few elements is refused before
+    any library call."""
+    import torch
+    from slak_b200 import api
+    ok_ids = torch.zeros(4, dtype=torch.int32)
+    for bad, err in ((dict(ids=torch.zeros(4, dtype=torch.int64)), TypeError),
+                     (dict(ids=torch.zeros(8, dtype=torch.int32)[::2]), TypeError),
+                     (dict(ids=ok_ids), TypeError),                                   # host memory
+                     (dict(verts=torch.zeros(16, dtype=torch.float64)), TypeError)):
+        dm = api.DeviceMesh(QUAD, 1, 4, 4, 4, True, **bad)
+        with pytest.raises(err):
+            dm.as_c()
+    assert api.DeviceMesh().as_c().ids is None                                       # an empty output is fine
