@@ -301,6 +301,8 @@ def subdivide_batched(meshes: List[DeviceMesh], levels: List[int], scheme: int, 
     """slak_subdivide_batched: every mesh refined in one call; each result owns
     its device arrays (freed with the returned DeviceMesh)."""
     n = len(meshes)
+    if len(levels) != n:
+        raise ValueError(f"subdivide_batched: {n} meshes but {len(levels)} level counts")
     arr = (_abi.SlakMesh * max(n, 1))()
     for i, m in enumerate(meshes):
         arr[i] = m.as_c()
@@ -324,6 +326,8 @@ class Batch:
     def __init__(self, meshes: List[DeviceMesh], levels: List[int], scheme: int, flags: int = 0, stream=None):
         self._meshes = list(meshes)
         n = len(self._meshes)
+        if len(levels) != n:
+            raise ValueError(f"Batch: {n} meshes but {len(levels)} level counts")
         self._arr = (_abi.SlakMesh * max(n, 1))()
         for i, m in enumerate(self._meshes):
             self._arr[i] = m.as_c()

@@ -51,3 +51,13 @@ def test_device_mesh_refuses_what_the_abi_would_misread():
         with pytest.raises(err):
             dm.as_c()
     assert api.DeviceMesh().as_c().ids is None                                       # an empty output is fine
+
+
+def test_batch_level_counts_must_match():
+    from slak_b200 import api
+    from slak_b200.mesh import SLAK
+    for levels in ([1], [1, 2, 3]):
+        with pytest.raises(ValueError):
+            api.subdivide_batched([api.DeviceMesh(), api.DeviceMesh()], levels, SLAK)
+        with pytest.raises(ValueError):
+            api.Batch([api.DeviceMesh(), api.DeviceMesh()], levels, SLAK)
