@@ -60,3 +60,37 @@ def test_meshgen_and_oracle_libraries_load():
     from slak_b200 import meshgen
     assert oracle.num_threads() >= 1
     assert meshgen.torus(4, 4).nfaces == 16
+
+
+def test_every_entry_point_checks_its_arguments_first(lib):
+    """Null handles, negative counts and unknown schemes give
+    SLAK_ERR_INVALID_ARG before any CUDA call (this runs with no GPU); the
+    destroy calls accept null, as free() does."""
+    m = _abi.SlakMesh()
+    m.type, m.nfaces, m.nnz, m.nverts = 1, 1, 4, 4
+    out = _abi.SlakMesh()
+    lv = (ctypes.c_int * 1)(1)
+    h = ctypes.c_void_p()
+    M, O = ctypes.byref(m), ctypes.byref(out)
+    calls = [
+        lambda: lib.slak_subdivide_batched(None, lv, 1, 1, O, None),
+        lambda: lib.slak_subdivide_batched(M, lv, -1, 1, O, None),
+        lambda: lib.slak_subdivide_batched(M, lv, 1, 9, O, None),
+        lambda: lib.slak_batch_create(None, lv, 1, 1, 0, None, ctypes.byref(h)),
+        lambda: lib.slak_batch_create(M, lv, 1, 1, 0, None, None),
+        lambda: lib.slak_subdivide_level_noalloc(None, None, 1, None),
+        lambda: lib.slak_subdivide_level_noalloc(M, O, 5, None),
+        lambda: lib.slak_plan_create_sharp(M, 1, 1, 0, None, None, -1, None, None, 0, None, ctypes.byref(h)),
+        lambda: lib.slak_plan_create_sharp(M, 1, 1, 0, None, None, 3, None, None, 0, None, ctypes.byref(h)),
+        lambda: lib.slak_obj_read(None, O),
+        lambda: lib.slak_obj_write(None, O),
+        lambda: lib.slak_plan_execute(None, None),
+        lambda: lib.slak_plan_status(None, None),
+        lambda: lib.slak_plan_output(None, O),
+        lambda: lib.slak_batch_execute(None, None),
+        lambda: lib.slak_batch_status(None, None),
+        lambda: lib.slak_batch_output(None, 0, O),
+    ]
+    for k, call in enumerate(calls):
+        assert call() == _abi.SLAK_ERR_INVALID_ARG, k
+    assert lib.slak_batch_destroy(None) == 0
