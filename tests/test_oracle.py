@@ -230,3 +230,37 @@ def test_unused_vertices_oracle(scheme):
     q1 = np.asarray(r1.ids, np.int64)
     expect = np.where(q0 < V0, shift(q0), q0 + 3)
     assert np.array_equal(q1, expect)
+
+
+def _with_positions(mesh, xyz):
+    v = np.ones((xyz.shape[0], 4), np.float32)
+    v[:, :3] = xyz
+    return Mesh(mesh.type, mesh.ids, v, mesh.ptr, mesh.vals, mesh.nfaces, mesh.max_face_order, mesh.is_reduced)
+
+
+def _props_cases():
+    from slak_b200 import meshgen
+    return [(n, m, lv) for n, m, lv in small_set()] + [
+        ("mixed", meshgen.mixed_torus(12, 10, 0.1, 0.05, 0.005, seed=4), 3),
+        ("open_grid", open_grid(6, 5), 3)]
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+@pytest.mark.parametrize("case", _props_cases(), ids=lambda c: c[0])
+def test_linear_and_affine(case, scheme):
+    """Refinement is a fixed linear map of the positions whose rows sum to 1
+    (every rule, boundary rules included, is an affine combination): in FP64,
+    S(P + Q) = S(P) + S(Q) and S(P + t) = S(P) + t.  Integer coordinates keep
+    the float32 inputs and their sums exact."""
+    name, mesh, levels = case
+    if scheme == LAK and mesh.ptr is None:
+        mesh = mesh.with_quad_ptr()
+    rng = np.random.default_rng(11)
+    V = mesh.nverts
+    P = rng.integers(-50, 50, (V, 3)).astype(np.float32)
+    Q = rng.integers(-50, 50, (V, 3)).astype(np.float32)
+    t = np.array([7.0, -3.0, 12.0], np.float32)
+    S = lambda X: oracle.subdivide(_with_positions(mesh, X), levels, scheme, fp64=True).verts64[:, :3]
+    sp, sq = S(P), S(Q)
+    assert np.abs(S(P + Q) - (sp + sq)).max() <= 1e-9
+    assert np.abs(S(P + t) - (sp + t)).max() <= 1e-9
