@@ -344,6 +344,14 @@ int obj_write(const char* path, const slak_mesh* m, const slak_creases* cr, cons
     if (!path || !m || m->nverts < 0 || m->nfaces < 0 || (m->nverts > 0 && !m->verts)) return SLAK_ERR_INVALID_ARG;
     const int fixed = m->type == SLAK_MESH_QUAD ? 4 : m->type == SLAK_MESH_TRI ? 3 : 0;
     if (m->nfaces > 0 && (!m->ids || (!fixed && !m->ptr))) return SLAK_ERR_INVALID_ARG;
+    // the faces are read through ptr / nnz: offsets that leave ids are refused
+    // before anything is written
+    if (fixed && m->nnz != (int64_t)fixed * m->nfaces) return SLAK_ERR_BAD_MESH;
+    if (!fixed && m->nfaces > 0) {
+        if (m->ptr[0] != 0 || (int64_t)m->ptr[m->nfaces] != m->nnz) return SLAK_ERR_BAD_MESH;
+        for (int64_t g = 0; g < m->nfaces; ++g)
+            if (m->ptr[g + 1] < m->ptr[g]) return SLAK_ERR_BAD_MESH;
+    }
     FILE* f = std::fopen(path, "wb");
     if (!f) return SLAK_ERR_INVALID_ARG;
     const int64_t V = m->nverts, F = m->nfaces;

@@ -205,3 +205,21 @@ def test_corner_tags_round_trip(tmp_path):
     r, (p2, s2), (k2, w2) = meshio.read_obj_sharp(str(path))
     assert np.array_equal(r.ids, m.ids) and np.array_equal(p2, pairs)
     assert np.array_equal(k2, kv) and np.array_equal(w2.view(np.uint32), ks.view(np.uint32))
+
+
+def test_writer_refuses_offsets_that_leave_ids(tmp_path):
+    """The writer reads faces through ptr / nnz: offsets that do not start at
+    0, do not end at nnz or go down, and a QUAD / TRI corner count that is not
+    4 or 3 per face, are refused (SLAK_ERR_BAD_MESH) before any byte is written."""
+    from slak_b200.mesh import Mesh
+    V = np.zeros((4, 4), np.float32)
+    ids = np.array([0, 1, 2, 0, 2, 3], np.int32)
+    for ptr in ([0, 3, 7], [1, 3, 6], [0, 4, 3, 6]):
+        m = Mesh(POLY, ids, V, np.array(ptr, np.int32), None, len(ptr) - 1, 3)
+        path = tmp_path / "w.obj"
+        with pytest.raises(_abi.SlakError) as e:
+            meshio.write_obj(str(path), m)
+        assert e.value.code == _abi.SLAK_ERR_BAD_MESH and not path.exists()
+    m = Mesh(QUAD, ids, V, None, None, 2, 4)                      # 6 corners for 2 quads
+    with pytest.raises(_abi.SlakError):
+        meshio.write_obj(str(tmp_path / "q.obj"), m)
