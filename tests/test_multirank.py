@@ -57,3 +57,31 @@ def test_two_gloo_ranks_time_and_partition():
     work = [sum(f * 4 ** (lv - 1) for _, f, lv, _ in sh) for sh in shards]
     biggest = max(f * 4 ** (lv - 1) for _, f, lv, _ in whole)
     assert abs(work[0] - work[1]) <= biggest                        # balanced to within one mesh
+
+
+@pytest.mark.parametrize("ws", [3, 4, 8])
+def test_partition_at_more_ranks(ws):
+    """The 2,000-mesh batch split over ws ranks (as `bench.py --gpus ws` does):
+    a partition, each shard in batch order, predicted work within one mesh."""
+    sys.path.insert(0, ROOT)
+    import bench
+    key = lambda it: (it.kind, it.faces, it.levels, it.seed)
+    whole = [key(it) for it in bench.batch_shard(2000)]
+    shards = [[key(it) for it in bench.batch_shard(2000, r, ws)] for r in range(ws)]
+    assert sorted(sum(shards, [])) == sorted(whole)
+    for sh in shards:
+        assert sh == [it for it in whole if it in set(sh)]
+    work = [sum(f * 4 ** (lv - 1) for _, f, lv, _ in sh) for sh in shards]
+    biggest = max(f * 4 ** (lv - 1) for _, f, lv, _ in whole)
+    assert max(work) - min(work) <= biggest
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under torchrun, `bench.py --impl reference` does its work on rank 0;
+    every other rank returns at once, with nothing to print."""
+    import argparse
+    sys.path.insert(0, ROOT)
+    import bench
+    args = argparse.Namespace(scheme="slak", workload="mixed512", steps=1, warmup=3, cpu_budget=1.0,
+                              crease_frac=0.0, batch_count=10)
+    assert bench.run_reference(args, None, 1, 2) is None
