@@ -95,6 +95,8 @@ def open_grid(W: int, H: int, jitter: float = 0.005, seed: int = 16) -> Mesh:
     """A flat W x H quad patch with height noise: an open mesh, its boundary a
     single loop of 2(W+H) edges (the boundary rules of both schemes)."""
     from .mesh import from_arrays
+    if W < 1 or H < 1:
+        raise ValueError(f"open_grid: W and H must be at least 1, got {W} x {H}")
     rng = np.random.default_rng(seed)
     i, j = np.meshgrid(np.arange(W + 1), np.arange(H + 1), indexing="ij")
     xyz = np.stack([i.ravel() / W, j.ravel() / H, jitter * rng.standard_normal(i.size)], 1)

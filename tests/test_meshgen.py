@@ -69,3 +69,15 @@ def test_batch_specs():
     assert 0.35 < kinds.count("torus") / 2000 < 0.45
     assert set(s.levels for s in specs) == {1, 2, 3, 4}
     assert meshgen.batch_specs(10) == meshgen.batch_specs(10)
+
+
+def test_degenerate_parameters_refused():
+    """Sizes a generator cannot build (a torus of fewer than 3 x 3 quads, an
+    icosphere of frequency < 1, a cylinder of < 3 segments or < 2 rings, an
+    empty grid) raise instead of returning a broken mesh."""
+    import pytest
+    for call in (lambda: meshgen.torus(0, 4), lambda: meshgen.torus(2, 2), lambda: meshgen.icosphere(0),
+                 lambda: meshgen.mixed_torus(0, 4), lambda: meshgen.capped_cylinder(2, 4),
+                 lambda: meshgen.capped_cylinder(8, 1), lambda: meshgen.open_grid(0, 3), lambda: meshgen.open_grid(4, 0)):
+        with pytest.raises(ValueError):
+            call()
