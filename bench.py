@@ -127,6 +127,20 @@ def _workload(name):
     return w.mesh, w.levels
 
 
+def _config(args, mesh, levels, faces, ws, creases=None):
+    """The `config` object of the JSON line, the same dict in both arms."""
+    return {"workload": f"{args.workload}: {mesh.nfaces} faces, {mesh.nverts} verts, {args.scheme.upper()}, "
+                        f"{levels} levels -> {faces} quads", "scheme": args.scheme.upper(),
+            "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
+            "parallelism": f"replicas x{ws}",
+            **({"creases": f"{creases[1].size} crease edges ({args.crease_frac:g} of the edges), "
+                           f"sharpness in {{0.5, 1, 2, 3, 5}}"} if creases is not None else {})}
+
+
+def _spread(ms):
+    return {"min": min(ms), "median": statistics.median(ms), "max": max(ms), "steps": len(ms)}
+
+
 def cpu_baseline(mesh, levels, scheme, budget_s=20.0, single_budget_s=10.0, creases=None):
     """The oracle (CPU restatement, OpenMP) on the largest prefix of levels that
     fits the budget; refined faces of that sample per second.  A single-thread
@@ -233,7 +247,7 @@ def run_ours(args, dist, rank, ws):
         _barrier(dist)
         st = plan.check(stream)
     ms = [a.elapsed_time(b) for a, b in ev]
-    spread = {"min": min(ms), "median": statistics.median(ms), "max": max(ms)}
+    spread = _spread(ms)
     ms_step = _max_over_ranks(dist, statistics.mean(ms))
     value = faces * ws / (ms_step * 1e-3)
     launches = plan.launches * args.steps
@@ -267,12 +281,7 @@ def run_ours(args, dist, rank, ws):
         "metric": "refined_faces_per_s", "value": value, "unit": "refined_faces/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{args.workload}: {mesh.nfaces} faces, {mesh.nverts} verts, {args.scheme.upper()}, "
-                               f"{levels} levels -> {faces} quads", "scheme": args.scheme.upper(),
-                   "levels": levels, "refined_faces": faces, "l2": "flushed (256 MiB write) before every step",
-                   "parallelism": f"replicas x{ws}",
-                   **({"creases": f"{creases[1].size} crease edges ({args.crease_frac:g} of the edges), "
-                                  f"sharpness in {{0.5, 1, 2, 3, 5}}"} if creases is not None else {})},
+        "config": _config(args, mesh, levels, faces, ws, creases),
         "gpu_launches": launches,
         "ms_per_step_spread": spread,
         "roofline": kern,
@@ -358,7 +367,7 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws, creases=None):
     d_cs = torch.empty_like(h_cs, device="cuda") if h_cs is not None else None
     h2d = sum(t.numel() * t.element_size() for t in (h_ptr, h_ids, h_vals, h_verts, h_cp, h_cs) if t is not None)
     d2h = 0
-    n = max(2, min(args.steps, 5))
+    n = max(2, args.steps)
     for i in range(args.warmup + n):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -386,29 +395,24 @@ def run_e2e(mesh, levels, scheme, args, torch, dist, ws, creases=None):
         if i >= args.warmup:
             times.append(dt)
     t = _max_over_ranks(dist, statistics.mean(times))
+    tm = _max_over_ranks(dist, statistics.median(times))
     return {"value": faces * ws / t, "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": t * 1e3,
-            "ms_spread": {"min": min(times) * 1e3, "median": statistics.median(times) * 1e3,
-                          "max": max(times) * 1e3, "steps": len(times)}}
+            "value_median": faces * ws / tm, "ms_per_step_median": tm * 1e3,
+            "ms_spread": _spread([x * 1e3 for x in times])}
 
 
 def batch_shard(count, rank=0, ws=1):
     """Specs of this rank's meshes of the 2,000-mesh batch (seeded kinds, sizes
-    and level counts), in batch order.  With ws > 1 the meshes are split by
-    predicted output (faces x 4^(levels-1), the refined quads up to a constant):
-    largest first, each to the rank with the least so far (ties to the lowest
-    rank), so every rank refines about the same number of quads."""
-    from slak_b200 import meshgen
+    and level counts), in batch order: the library's partition
+    (slak_b200.shard) by predicted output, faces x 4^(levels-1), so the specs
+    are split before any geometry is generated."""
+    from slak_b200 import meshgen, shard
     specs = meshgen.batch_specs(count)
     if ws == 1:
         return specs
-    load = [0] * ws
-    owner = [0] * len(specs)
-    for k in sorted(range(len(specs)), key=lambda k: (-specs[k].faces * 4 ** (specs[k].levels - 1), k)):
-        r = min(range(ws), key=lambda r: (load[r], r))
-        owner[k] = r
-        load[r] += specs[k].faces * 4 ** (specs[k].levels - 1)
-    return [it for k, it in enumerate(specs) if owner[k] == rank]
+    work = [it.faces * 4 ** (it.levels - 1) for it in specs]
+    return [specs[k] for k in shard.shard_indices(work, rank, ws)]
 
 
 def batch_workload(count, rank=0, ws=1):
@@ -580,8 +584,10 @@ def run_reference_batch(args, scheme):
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
         "config": {"workload": f"batch{args.batch_count}: per-mesh loop, {'SLAK' if scheme else 'LAK'}",
                    "parallelism": "replicas x1"},
-        "cpu_baseline": {"value": value, "unit": "refined_faces/s", "cores": 1, "kind": "reference",
-                         "sample": sample},
+        "path": "GPUPeople/SLAK's own CUDA path, one subdivideIteratively per mesh",
+        "cpu_baseline": {"value": None, "unit": "refined_faces/s", "cores": 0, "kind": "reference",
+                         "unavailable": "the reference has no CPU implementation of the path; this line times "
+                                        "its CUDA path", "sample": sample},
         "e2e": {"value": value, "unit": "refined_faces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clk.summary(),
     }
@@ -610,29 +616,29 @@ def run_reference(args, dist, rank, ws):
     faces = sizes[-1][2]
     ms_step = statistics.mean(ms)
     value = faces / (ms_step * 1e-3)
-    spread = {"min": min(ms), "median": statistics.median(ms), "max": max(ms)}
     # end to end through the reference's public call with host buffers: the
-    # same pinned H2D of the input and D2H of the refined ids and positions as
-    # this repository's e2e figure
-    e2e_ms, h2d, d2h = ref.time_e2e(mesh, levels, scheme, 1, max(2, min(args.steps, 5)))
-    e2e_t = statistics.mean(e2e_ms)
+    # same pinned H2D of the input and D2H of the refined ids and positions,
+    # over the same number of steps, as this repository's e2e figure
+    e2e_ms, h2d, d2h = ref.time_e2e(mesh, levels, scheme, 1, max(2, args.steps))
+    e2e_t, e2e_med = statistics.mean(e2e_ms), statistics.median(e2e_ms)
     return {
         "impl": "reference", "metric": "refined_faces_per_s", "value": value, "unit": "refined_faces/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": f"{args.workload}: {mesh.nfaces} faces, {args.scheme.upper()}, {levels} levels -> "
-                               f"{faces} quads", "scheme": args.scheme.upper(), "levels": levels,
-                   "refined_faces": faces, "parallelism": "replicas x1"},
+        "config": _config(args, mesh, levels, faces, ws),
         "reference_self_reported_ms": statistics.mean(self_ms) if self_ms else None,
-        "ms_per_step_spread": spread,
-        "cpu_baseline": {"value": value, "unit": "refined_faces/s", "cores": 1, "kind": "reference",
-                         "sample": "GPUPeople/SLAK's own CUDA path (built for sm_100a) on the full workload; "
-                                   "the reference has no CPU implementation"},
+        "ms_per_step_spread": _spread(ms),
+        "path": "GPUPeople/SLAK's own CUDA path (subdivideIteratively, built for sm_100a from its sources), "
+                "device-resident input",
+        "cpu_baseline": {"value": None, "unit": "refined_faces/s", "cores": 0, "kind": "reference",
+                         "unavailable": "the reference has no CPU implementation of the path; this line times "
+                                        "its CUDA path (the CPU restatement is timed in the repository's arm)",
+                         "sample": "none"},
         "e2e": {"value": faces / (e2e_t * 1e-3), "unit": "refined_faces/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_t,
-                "ms_spread": {"min": min(e2e_ms), "median": statistics.median(e2e_ms), "max": max(e2e_ms),
-                              "steps": len(e2e_ms)}},
+                "value_median": faces / (e2e_med * 1e-3), "ms_per_step_median": e2e_med,
+                "ms_spread": _spread(e2e_ms)},
         "clocks": clk.summary(),
     }
 

@@ -3,9 +3,11 @@
 //
 // Same names and shapes: struct CatmullClark with the nested
 // MeshInfo<OFFSET, INDEX, VALUE, VERTEX> (CatmullClark.h:69-130 of the
-// reference) and the static template subdivideIteratively
-// (CatmullClark.h:163-164), usable for MeshInfo<int, int, int, float> (the only
-// instantiation the reference provides, CatmullClarkImpl.cu:520-522).  The
+// reference, freeAndReset() and freeAndReset(MEM_MANAGER&) included),
+// Context<MESH_INFO> (:38-59), ProfilinInfo<PROFILER, MEM_MANAGER> (:62-67)
+// and the static template subdivideIteratively (CatmullClark.h:163-164),
+// usable for MeshInfo<int, int, int, float> (the only instantiation the
+// reference provides, CatmullClarkImpl.cu:520-522).  The
 // work runs in libslak_b200.so through the C ABI of slak_b200.h.
 //
 // Behaviour kept from the reference: device-resident input that is never
@@ -32,6 +34,15 @@ inline void succeed(cudaError_t e)
         std::printf("CUDA ERROR: %s", cudaGetErrorString(e));
         throw(cudaGetErrorString(e));
     }
+}
+
+// MeshInfo::freeAndReset(mem): the manager frees what it allocated
+// (freeMemory returns true); anything else came from cudaMalloc
+template <class MEM, class T>
+void release(MEM& mem, T*& p)
+{
+    if (p != nullptr && !mem.freeMemory(p)) succeed(cudaFree(p));
+    p = nullptr;
 }
 
 template <class MI>
@@ -117,10 +128,52 @@ void run(const MI& cmesh, MI& rmesh, int target_level, int scheme, const char* b
             if (verts != nullptr) slak_b200_detail::succeed(cudaFree(verts));                      \
             *this = MeshInfo();                                                                    \
         }                                                                                          \
+        /* each array goes to mem.freeMemory(p) first; one the manager did */                     \
+        /* not hand out (it returns false) is cudaFree'd                    */                     \
+        template <typename MEM_MANAGER>                                                            \
+        void freeAndReset(MEM_MANAGER& mem)                                                        \
+        {                                                                                          \
+            slak_b200_detail::release(mem, ptr);                                                   \
+            slak_b200_detail::release(mem, ids);                                                   \
+            slak_b200_detail::release(mem, vals);                                                  \
+            slak_b200_detail::release(mem, verts);                                                 \
+            *this = MeshInfo();                                                                    \
+        }                                                                                          \
+    };
+
+// The reference's per-scheme scratch record (Context) and its pairing of a
+// profiler with a memory manager (ProfilinInfo) are public nested types of
+// each scheme's struct.  This library keeps its scratch in a plan and never
+// reads a Context; the types exist so that host code naming them compiles.
+#define SLAK_B200_PROFILININFO                                                                     \
+    template <typename PROFILER_TYPE, typename MEM_MANAGER_TYPE>                                   \
+    struct ProfilinInfo {                                                                          \
+        PROFILER_TYPE prof;                                                                        \
+        MEM_MANAGER_TYPE mem;                                                                      \
     };
 
 struct CatmullClark
 {
+    // field names and defaults of the reference's CatmullClark::Context
+    // (CatmullClark.h:38-59): adjacency, ordering and mapping buffers and the
+    // boundary bookkeeping of its implementation; unused here
+    template <typename MESH_INFO>
+    struct Context {
+        using index_t = typename MESH_INFO::index_t;
+        size_t block_dim{256};
+        bool is_initialized{false};
+        index_t* d_order_buffer{nullptr};
+        index_t* d_S_buffer{nullptr};
+        index_t* d_mapping_buffer{nullptr};
+        index_t* d_face_adjacency{nullptr};
+        bool has_boundary{true};
+        index_t nextern{0};
+        index_t* d_nextern{nullptr};
+        index_t* d_vextern{nullptr};
+    };
+
+    SLAK_B200_PROFILININFO
+
     SLAK_B200_MESHINFO
 
     template<typename MESH_INFO>

@@ -173,9 +173,13 @@ int slak_mesh_free(slak_mesh* mesh);
  * On success, the counts in *rmesh are set as slak_subdivide sets them.
  *
  * The scratch is a fixed 32 MiB device array inside this library.  Every GPU
- * that loads the library holds it until the process exits.  Meshes whose
- * scratch does not fit are rejected with SLAK_ERR_UNSUPPORTED (about
- * 500k corners).  All calls share that array:
+ * that loads the library holds it until the process exits.  A level needs
+ * 36 bytes of scratch per corner (40 for a non-QUAD cmesh) plus 16 per vertex,
+ * each of its 13-14 arrays rounded up to 256 bytes, plus its scan tiles
+ * (4 bytes per 2048 corners) and a status record; meshes whose scratch does
+ * not fit are rejected with SLAK_ERR_UNSUPPORTED before anything runs.  That
+ * is about 830k corners for a closed quad mesh (vertices = corners / 4).
+ * All calls share that array:
  *   - calls that overlap on the GPU (two streams, or two host threads) race,
  *     so serialise them;
  *   - each call clears what must start at zero.

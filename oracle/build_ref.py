@@ -8,7 +8,7 @@ are compiled directly, with ref_shim.h force-included to stand in for the
 legacy texture reference CUDA 12 removed (used only by the disabled
 EXPLICIT_MAP_LOOKUP multiply of LibInclude/device/math/spgemm.cuh).
 
-    python oracle/build_ref.py [/root/reference]
+    python oracle/build_ref.py REFERENCE_DIR       (or $SLAK_REFERENCE_ROOT)
 """
 from __future__ import annotations
 
@@ -88,7 +88,9 @@ def build_dropin_main(ref_root: str, out_dir: str, include_dir: str, lib_dir: st
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SLAK_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: python oracle/build_ref.py REFERENCE_DIR (or set SLAK_REFERENCE_ROOT)")
     print(build(root, os.path.join(HERE, "_ref"), verbose=True, force=True))
     repo = os.path.dirname(HERE)
     print(build_dropin_main(root, os.path.join(HERE, "_ref"), os.path.join(repo, "include"),

@@ -169,19 +169,25 @@ int ref_run(int scheme, const ref_mesh* in, int levels, ref_mesh* out, float* se
 
 // Times `reps` calls on device-resident input: ms_each[i] brackets one
 // subdivideIteratively with CUDA events (output freed outside the bracket);
-// self_ms[i] is the reference's own printed "took X ms".
+// self_ms[i] is the reference's own printed "took X ms".  Before every call,
+// outside the bracket, 256 MiB are written to flush L2, as the repository's
+// own timing does.
 int ref_time(int scheme, const ref_mesh* in, int levels, int warmup, int reps, double* ms_each, float* self_ms,
              int quiet)
 {
     DevInput d;
     int rc = d.upload(*in);
     if (rc) return rc;
+    const size_t flush_bytes = size_t(256) << 20;
+    void* flush = nullptr;
+    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) return 3;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     StdoutCapture cap(quiet != 0);      // one redirect around the whole loop
     for (int i = -warmup; i < reps && !rc; ++i) {
         float ms = 0.f;
+        cudaMemsetAsync(flush, i & 0xff, flush_bytes);
         cudaEventRecord(a);
         if (scheme == 1) {
             CatmullClark::MeshInfo<int, int, int, float> r;
@@ -211,6 +217,7 @@ int ref_time(int scheme, const ref_mesh* in, int levels, int warmup, int reps, d
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    cudaFree(flush);
     return rc;
 }
 

@@ -7,11 +7,11 @@ the mesh container and the seeded workload generators.
 """
 from .mesh import LAK, POLY, QUAD, SLAK, TRI, Mesh  # noqa: F401
 
-__all__ = ["Mesh", "LAK", "SLAK", "TRI", "QUAD", "POLY", "api", "meshgen", "canon"]
+__all__ = ["Mesh", "LAK", "SLAK", "TRI", "QUAD", "POLY", "api", "meshgen", "canon", "shard"]
 
 
 def __getattr__(name):
     import importlib
-    if name in ("api", "meshgen", "canon", "build", "_abi"):
+    if name in ("api", "meshgen", "canon", "build", "_abi", "shard"):
         return importlib.import_module(f".{name}", __name__)
     raise AttributeError(name)

@@ -94,10 +94,13 @@ def build_oracle(verbose=False, force=False):
     return _paths.LIB_ORACLE
 
 
-def build_reference(verbose=False, force=False, ref_root="/root/reference"):
+def build_reference(verbose=False, force=False, ref_root=None):
     """Compiles the reference's CUDA sources (never copied) with oracle/build_ref.py,
-    and the reference's driver against the drop-in headers (oracle/_ref/slak_main_dropin)."""
-    if not os.path.isdir(ref_root):
+    and the reference's driver against the drop-in headers (oracle/_ref/slak_main_dropin).
+    The reference tree is `ref_root`, else $SLAK_REFERENCE_ROOT; with neither
+    (or no such directory) nothing is built and None is returned."""
+    ref_root = ref_root or os.environ.get("SLAK_REFERENCE_ROOT")
+    if not ref_root or not os.path.isdir(ref_root):
         return None
     sys.path.insert(0, _paths.REPO_DIR)
     try:
@@ -110,14 +113,16 @@ def build_reference(verbose=False, force=False, ref_root="/root/reference"):
     return out
 
 
-def build_all(verbose=False, force=False):
+def build_all(verbose=False, force=False, ref_root=None):
     build_meshgen(verbose, force)
     build_cuda(verbose, force)
     build_demo(verbose, force)
     build_oracle(verbose, force)
-    build_reference(verbose, force)
+    build_reference(verbose, force, ref_root)
 
 
 if __name__ == "__main__":
-    build_all(verbose="-v" in sys.argv, force="-f" in sys.argv)
+    # python -m slak_b200.build [-v] [-f] [--reference DIR]
+    ref = sys.argv[sys.argv.index("--reference") + 1] if "--reference" in sys.argv else None
+    build_all(verbose="-v" in sys.argv, force="-f" in sys.argv, ref_root=ref)
     print("built:", _paths.LIB_SLAK)

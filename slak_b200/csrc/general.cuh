@@ -70,7 +70,10 @@ __global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restr
 }
 
 // slot order from the atomic is arbitrary (the unsorted column goes to
-// `loose`); k_vsort makes it canonical
+// `loose`); k_vsort makes it canonical.  A malformed polygon mesh (a face the
+// valence pass rejected, or corners past ptr[F]) brings more corners to a
+// vertex than its column counts: those find no slot (r < 0) and are dropped,
+// so nothing is written outside the column; the level fails with BAD_MESH.
 __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
                          int* __restrict__ fill, int* __restrict__ loose)
 {
@@ -79,7 +82,7 @@ __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* _
     int v = ids[c];
     if ((unsigned)v >= (unsigned)V) return;
     int r = atomicSub(fill + v, 1) - 1;
-    loose[sptr[v] + r] = c;
+    if (r >= 0) loose[sptr[v] + r] = c;
 }
 
 // Each column sorted by corner index: a corner's slot is the number of smaller

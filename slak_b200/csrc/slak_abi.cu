@@ -1810,10 +1810,17 @@ extern "C" int slak_subdivide_level_noalloc(const slak_mesh* cm, slak_mesh* rm, 
     cudaMemcpyAsync(&nedges, s.eptr + V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
     if (e != cudaSuccess) return cuda_status(e);
-    if (h.err) return h.err;
+    if (h.err) {
+        g_detail = "level 0 topology: detail " + std::to_string(h.detail);
+        return h.err;
+    }
     L.B = h.bcount[0];
     L.E = nedges;
-    if (L.E != (N - L.B) / 2 + L.B) return SLAK_ERR_BAD_MESH;
+    if (L.E != (N - L.B) / 2 + L.B) {
+        g_detail = "level 0 has " + std::to_string(L.E) + " edges and " + std::to_string(L.B) +
+                   " boundary half-edges: not a manifold mesh";
+        return SLAK_ERR_BAD_MESH;
+    }
     L.Fo = N; L.No = 4 * N; L.Vo = V + F + L.E;
     if (rm->nverts < L.Vo) {      // rm->nverts carries the capacity of rm->verts, in vertices
         g_detail = "output positions need " + std::to_string(L.Vo) + " vertices";
@@ -1825,11 +1832,20 @@ extern "C" int slak_subdivide_level_noalloc(const slak_mesh* cm, slak_mesh* rm, 
     if (quad) launch_rest<true>(L, 0, scheme, false, s, st, lc);
     else launch_rest<false>(L, 0, scheme, false, s, st, lc);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
+    if (e != cudaSuccess) {
+        // kernels of this call that did launch may still use the array: the
+        // call returns only once the stream is idle, so the next call cannot race them
+        cudaStreamSynchronize(str);
+        g_detail = std::string("launch: ") + cudaGetErrorString(e);
+        return cuda_status(e);
+    }
     cudaMemcpyAsync(&h, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
     if (e != cudaSuccess) return cuda_status(e);
-    if (h.err) return h.err;
+    if (h.err) {
+        g_detail = "level 0: detail " + std::to_string(h.detail);
+        return h.err;
+    }
     rm->type = SLAK_MESH_QUAD;
     rm->nfaces = L.Fo; rm->nnz = L.No; rm->nverts = L.Vo;
     rm->is_reduced = lak ? 0 : 1;

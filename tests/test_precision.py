@@ -43,7 +43,7 @@ def _timed(mesh, levels, scheme, flags, reps=5):
     return out, ms, faces
 
 
-CASES = {"cylinder": ("capped cylinder 64x32, valence-64 poles, jitter 0.001", {SLAK: 7, LAK: 6}),
+CASES = {"cylinder": ("capped cylinder 64x32, valence-64 poles, jitter 0.001", {SLAK: 7, LAK: 7}),
          "mixed512": ("512x512 mixed-polygon torus (n-gons 3-8, valence 3-10), jitter 0.005", {SLAK: 4, LAK: 4})}
 
 

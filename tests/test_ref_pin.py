@@ -55,3 +55,15 @@ def test_reference_matches_oracle_small(case, scheme):
 def test_reference_matches_oracle_workloads(name, levels, scheme):
     _ref_or_skip()
     _compare(meshgen.workload(name).mesh, levels, scheme)
+
+
+@pytest.mark.parametrize("scheme", [LAK, SLAK])
+def test_reference_matches_oracle_mixed_polygons(scheme):
+    """The large mixed-polygon workload's structure (5% of face pairs merged,
+    3% of quads split: n-gons of 3-8 sides, valence 3-10, closed) at 128 x 128,
+    3 levels: the reference's own output against the oracle."""
+    _ref_or_skip()
+    mesh = meshgen.mixed_torus(128, 128, 0.05, 0.03, 0.005)
+    order = np.diff(mesh.ptr)
+    assert order.min() == 3 and order.max() >= 6
+    _compare(mesh, 3, scheme)
