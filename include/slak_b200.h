@@ -210,7 +210,9 @@ enum slak_plan_flags {
     SLAK_PLAN_GENERAL = 2,      /* run every level through the general per-level path         */
     SLAK_PLAN_COMPENSATED = 4,  /* compensated (TwoSum) sums in high-valence vertex points    */
     SLAK_PLAN_TIMING = 8,       /* record a CUDA event after every launch (per-kernel times)  */
-    SLAK_PLAN_AUTOTUNE = 16     /* measure launch shapes of untuned keys at creation (below)  */
+    SLAK_PLAN_AUTOTUNE = 16,    /* measure launch shapes of untuned keys at creation (below)  */
+    SLAK_PLAN_GQ = 32           /* grandparent-quad levels: k_g1 sums most of the parent's    */
+                                /* vertex columns instead of k_g3 (same results)             */
 };
 
 typedef struct slak_kernel_timing {

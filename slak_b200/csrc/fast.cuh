@@ -57,6 +57,7 @@ struct FastDims {
     int N1, V1, F1, E1;    // P
     int V, N;              // C (F = N1, E = 2 N1 + B1)
     int B1;                // P's boundary edges (0: closed)
+    int N2 = 0, V2 = 0, F2 = 0;   // GQ levels: P's parent PP (a closed quad mesh)
 };
 
 __device__ __forceinline__ float4 shfl4_xor(float4 v, int m)
@@ -76,15 +77,25 @@ __device__ __forceinline__ void st_pos(float* R, int64_t i, float4 v)
     else st4_cs(R, i, v);
 }
 
-// The slot records k_g1 writes and k_g3 reads back once, stored with an L2
-// evict-last policy.  Measured on B200 (512x512 mixed torus, SLAK), this
-// takes k_g1's last level from 641 to 619 us; k_g3's time does not move.
-__device__ __forceinline__ void st4_keep(float4* p, float4 v)
+// A slot record {face point, neighbour} (Z[2s], Z[2s+1]: 32 bytes, 32-byte
+// aligned), written by k_g1 and read back once by k_g3, moves as one 256-bit
+// access (sm_100's widest vector load / store): one L1 wavefront per lane
+// instead of two.  The store carries an L2 evict-last policy (measured on
+// B200, 512x512 mixed torus, SLAK: k_g1's last level 641 -> 619 us, k_g3's
+// time unchanged); the load is a read-only (non-coherent) one, as __ldg.
+__device__ __forceinline__ void st8_keep(float4* p, float4 a, float4 b)
 {
     uint64_t pol;
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
-                 :: "l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol));
+    asm volatile("st.global.L2::cache_hint.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8}, %9;"
+                 :: "l"(p), "f"(a.x), "f"(a.y), "f"(a.z), "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w),
+                    "l"(pol));
+}
+__device__ __forceinline__ void ld8_nc(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
 }
 
 // rank of corner `a` among the four corners of an edge point
@@ -236,6 +247,158 @@ __device__ __forceinline__ void boundary_edge(const FastDims& d, QState& c, floa
     if (STATE) c.sptr[ve] = 2 * d.N1 + 4 * e - 2 * br;
 }
 
+// ---------------------------------------------------------------------------------------------
+// GQ: P = refine(PP) with PP a closed quad mesh (N2 corners, V2 vertices, F2 =
+// N2 / 4 faces), so P corner x = 4y + k is corner k of P face y = PP corner y,
+// and the 16 lanes 16g..16g+15 hold the P corners of PP face g.  Two kinds of
+// P's vertex columns then lie inside those lanes, and k_g1 computes their
+// vertex points (and SLAK edge points) without slot records; k_g3 keeps PP's
+// old vertices (slots below N2) only.
+//   PP face point V2 + g: corners 16g + 4j + 2 (j = 0..3, column order),
+//     slots N2 + 4g + j; SLAK edge slot N2 + 4g + j pairs quad j with quad j-1.
+//     The lane of j = 0 sums the column; each of the four lanes its edge point.
+//   PP edge point V2 + F2 + e, with PP half-edges h: v -> u (v < u) and h2:
+//     corners A = 4h+1 (this lane), B = 4 next(h) + 3 (same group),
+//     C2 = 4 h2 + 1, D2 = 4 next(h2) + 3 (the twin's group).  C quads C2 and D2
+//     are {ve, X, V1 + h2, e_out(B)} and {ve, e_out(4h), V1 + next(h2), X}: X,
+//     C's vertex on the P edge between P faces h2 and next(h2), is V1 + F1 +
+//     N2 + next(h2) (SLAK) or V1 + F1 + 4e + 2 + [face(h2) > face(h)] (LAK),
+//     and next(h2) comes from P's twin of 4h, 4 next(h2) + 3.  So three gathers
+//     (X and two of P's face points) rebuild both face points.  SLAK's four
+//     edges around ve pair A-B, B-C2, C2-D2, D2-A; their ids are 2 N2 + 4e +
+//     the quad's rank in the column.
+// Sums and their order are k_g3's (column order; LAK tails by ascending id).
+template <bool LAK, bool STATE>
+__device__ __forceinline__ void gq_columns(const FastDims& d, QState& c, const float* __restrict__ P,
+                                           float* __restrict__ R, bool valid, int x, int lane, const int4& Q,
+                                           int tw1x, float4 c0, float4 c1, float4 c3, float4 fp)
+{
+    const unsigned full = 0xffffffffu;
+    const int k = x & 3, j = (x >> 2) & 3;
+    const int g16 = lane & ~15;                    // lane of P corner 16g
+    const int l0 = lane & ~3;                      // lane of P corner 4y (y = x >> 2)
+    const int ln = g16 | (((j + 1) & 3) << 2);     // lane of P corner 4 next(y)
+    const int lB = ln | 3;                         // lane of P corner 4 next(y) + 3
+    const int tail = __shfl_sync(full, Q.x, l0);  // PP vertex of corner y
+    const int head = __shfl_sync(full, Q.x, ln);  // PP vertex of corner next(y)
+    const int tw0 = __shfl_sync(full, tw1x, l0);  // P's twin of 4y: 4 next(h2) + 3
+    const bool fw = valid && k == 2 && j == 0;     // sums PP face point (Q.x)'s column
+    const bool ew = valid && k == 1 && tail < head;   // sums PP edge point (Q.x)'s column
+    // sources of the exchanges, in column order for the face point's lane
+    int src[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) src[r] = fw ? g16 | (r << 2) | 2 : lane;
+    if (ew) { src[0] = lB; src[1] = l0; }
+    if (!fw && !ew && k == 2) src[0] = g16 | (((j + 3) & 3) << 2) | 2;   // the previous quad's face point
+    // the values from the edge point's own group: e_out of quads B and 4y, and B's face point
+    float4 c1B, c1h0, fpB;
+    float4 yv = f4_zero();                         // the face point's vertex point, summed as values arrive
+    if (!LAK) {
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float4 t = shfl4(c1, src[r]);
+            acc = f4_add(acc, t);
+            if (r == 0) c1B = t;
+            if (r == 1) c1h0 = t;
+        }
+        yv = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(c0, 2.0f), 4.0f));
+        float4 fprev = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float4 t = shfl4(fp, src[r]);
+            yv = f4_add(yv, f4_div(t, 16.0f));
+            if (r == 0) { fpB = t; fprev = t; }
+            if (r == 3 && j == 0) fprev = t;
+        }
+        if (valid && k == 2) {                     // SLAK edge point of slot N2 + y: quads j and j - 1
+            const float4 ta = f4_mul(f4_add(c0, fp), 0.25f);
+            st4_cs(R, (int64_t)d.V + d.N1 + d.N2 + (x >> 2),
+                   f4_add(f4_add(f4_zero(), ta), f4_mul(f4_add(c1, fprev), 0.25f)));
+        }
+    } else {
+        // the face point's column: face points in column order, then the tails
+        // (e_in) in ascending id; the edge point's lane takes B's values
+        int tid[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) tid[r] = __shfl_sync(full, Q.w, src[r]);
+        const int qyB = __shfl_sync(full, Q.y, lB);
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float4 t = shfl4(fp, src[r]);
+            acc = f4_add(acc, t);
+            if (r == 0) fpB = t;
+        }
+        float4 c3B;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {              // source of rank r (the edge point's lane: B)
+            int sr = src[0];
+#pragma unroll
+            for (int i = 1; i < 4; ++i)
+                if (rank4(tid[i], tid[(i + 1) & 3], tid[(i + 2) & 3], tid[(i + 3) & 3]) == r) sr = src[i];
+            if (rank4(tid[0], tid[1], tid[2], tid[3]) == r) sr = src[0];
+            const float4 t = shfl4(c3, fw ? sr : (r == 0 ? lB : lane));
+            acc = f4_add(acc, t);
+            if (r == 0) c3B = t;
+        }
+        yv = f4_div_z(f4_add(f4_div_z(acc, 4.0f), f4_mul(c0, 2.0f)), 4.0f);
+        c1B = shfl4(c1, lB);
+        c1h0 = shfl4(c1, l0);
+        if (ew) {
+            const int y = x >> 2, nh2 = tw0 >> 2, h2 = qprev(nh2);
+            const int e = Q.x - d.V2 - d.F2;
+            const int X = d.V1 + d.F1 + 4 * e + 2 + ((h2 >> 2) > (y >> 2));
+            const float4 PX = ldg4(P, X), Pf2 = ldg4(P, d.V1 + h2), Pfn2 = ldg4(P, d.V1 + nh2);
+            const float4 fC2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), PX), Pf2), c1B), 4.0f);
+            const float4 fD2 = f4_div_z(f4_add(f4_add(f4_add(f4_add(f4_zero(), c0), c1h0), Pfn2), PX), 4.0f);
+            const int cA = x, cB = 4 * (y & ~3 | ((y + 1) & 3)) + 3, cC = 4 * h2 + 1, cD = 4 * nh2 + 3;
+            const int rA = rank4(cA, cB, cC, cD), rB = rank4(cB, cA, cC, cD), rC = rank4(cC, cA, cB, cD);
+            float4 a2 = f4_zero();
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a2 = f4_add(a2, rA == r ? fp : rB == r ? fpB : rC == r ? fC2 : fD2);
+            // tails e_in of A, B, C2, D2 = c3, c3B, c1B, PX with ids Q.w, Q.w(B), Q.y(B), X
+            const int tA = Q.w, tB = tid[0], tC = qyB, tD = X;
+            const int sA = rank4(tA, tB, tC, tD), sB = rank4(tB, tA, tC, tD), sC = rank4(tC, tA, tB, tD);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a2 = f4_add(a2, sA == r ? c3 : sB == r ? c3B : sC == r ? c1B : PX);
+            yv = f4_div_z(f4_add(f4_div_z(a2, 4.0f), f4_mul(c0, 2.0f)), 4.0f);
+        }
+    }
+    if (fw || (LAK && ew)) {
+        st_pos<STATE>(R, Q.x, yv);
+        if (STATE) c.sptr[Q.x] = fw ? d.N2 + (x >> 2) : 2 * d.N2 + 4 * (Q.x - d.V2 - d.F2);
+    }
+    if (!LAK && ew) {
+        const int y = x >> 2, nh2 = tw0 >> 2, h2 = qprev(nh2);
+        const int e = Q.x - d.V2 - d.F2;
+        const int X = d.V1 + d.F1 + d.N2 + nh2;
+        const float4 PX = ldg4(P, X), Pf2 = ldg4(P, d.V1 + h2), Pfn2 = ldg4(P, d.V1 + nh2);
+        const float4 fC2 = f4_mul(f4_add(f4_add(c0, Pf2), f4_add(PX, c1B)), 0.25f);
+        const float4 fD2 = f4_mul(f4_add(f4_add(c0, Pfn2), f4_add(c1h0, PX)), 0.25f);
+        // the column's quads A, B, C2, D2 (neighbour e_out, face point) and their ranks
+        const int cA = x, cB = 4 * (y & ~3 | ((y + 1) & 3)) + 3, cC = 4 * h2 + 1, cD = 4 * nh2 + 3;
+        const int rA = rank4(cA, cB, cC, cD), rB = rank4(cB, cA, cC, cD), rC = rank4(cC, cA, cB, cD);
+        float4 acc = f4_zero();
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc = f4_add(acc, rA == r ? c1 : rB == r ? c1B : rC == r ? PX : c1h0);
+        float4 ye = f4_add(f4_div(acc, 16.0f), f4_div(f4_mul(c0, 2.0f), 4.0f));
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ye = f4_add(ye, f4_div(rA == r ? fp : rB == r ? fpB : rC == r ? fC2 : fD2, 16.0f));
+        st_pos<STATE>(R, Q.x, ye);
+        if (STATE) c.sptr[Q.x] = 2 * d.N2 + 4 * e;
+        // edges around ve, at the column's slots: quad A with B, B with C2, C2 with D2, D2 with A
+        const int64_t eb = (int64_t)d.V + d.N1 + 2 * (int64_t)d.N2 + 4 * (int64_t)e;
+        const auto ep = [&](float4 f, float4 nb, float4 fn) {
+            return f4_add(f4_add(f4_zero(), f4_mul(f4_add(c0, f), 0.25f)), f4_mul(f4_add(nb, fn), 0.25f));
+        };
+        st4_cs(R, eb + rA, ep(fp, c1, fpB));
+        st4_cs(R, eb + rB, ep(fpB, c1B, fC2));
+        st4_cs(R, eb + rC, ep(fC2, PX, fD2));
+        st4_cs(R, eb + (6 - rA - rB - rC), ep(fD2, c1h0, fp));
+    }
+}
+
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
@@ -244,8 +407,8 @@ __device__ __forceinline__ void boundary_edge(const FastDims& d, QState& c, floa
 // optr / ovals (LAK, last level): the refined mesh's ptr[q] = 4q and
 // vals[q] = {1, 2, 3, 4}; they depend on q alone, so a block writes the 4 BS
 // refined quads of its span with consecutive threads (coalesced).
-template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
-__global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false>
+__global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
                                            int* __restrict__ optr, int4* __restrict__ ovals)
@@ -361,11 +524,15 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
 
     if (valid) {
         st_pos<STATE>(R, (int64_t)d.V + x, fp);
-        // records of corner x for its vertex's pass (full 32-byte sectors at slot s1)
-        st4_keep(z.Z + 2 * (int64_t)s1, fp);
-        st4_keep(z.Z + 2 * (int64_t)s1 + 1, LAK ? c3 : c1);
+    }
+    // records of corner x for its vertex's pass (full 32-byte sectors at slot
+    // s1); with GQ only the corners at PP's old vertices (q == 0) have them
+    if (valid && (!GQ || q == 0)) {
+        st8_keep(z.Z + 2 * (int64_t)s1, fp, LAK ? c3 : c1);
         if (LAK) z.T[s1] = Q.w;
         else if (!BND || t1x >= 0) z.rot[t1x] = s1;
+    }
+    if (valid) {
         if (BND && !LAK && tw1x < 0) z.rot[s1] = s1;      // no rotation across the boundary: a safe index
         if (BND) {
             z.bflag[s1] = (tw1x < 0) | ((tw1_px < 0) << 1);
@@ -459,6 +626,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_g1(FastDims d, Faces<PQ> pf, 
             edge_point_vertex<LAK, STATE, BND>(d, c, R, x, nxx, h2, nh2, Q.y, Q.z, fh2, c0, Pu, c1, c2, Pf2, fp,
                                                Fnh, Fh2, Fnh2, br_x);
         }
+        if constexpr (GQ) gq_columns<LAK, STATE>(d, c, P, R, valid, x, lane, Q, tw1x, c0, c1, c3, fp);
     }
     if (LAK && !STATE && optr != nullptr) {
         const int64_t q0 = 4 * (int64_t)x0;
@@ -721,8 +889,7 @@ __device__ __forceinline__ void g3_vertex(FastDims d, const float* __restrict__ 
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k < n) {
-                zf[k] = __ldg(Z + 2 * (int64_t)(b + k));
-                zn[k] = __ldg(Z + 2 * (int64_t)(b + k) + 1);
+                ld8_nc(Z + 2 * (int64_t)(b + k), zf[k], zn[k]);
                 tt[k] = LAK ? __ldg(z.T + b + k) : __ldg(z.rot + b + k) - b;
                 if (BND) fl[k] = __ldg(z.bflag + b + k);
             }
@@ -847,6 +1014,7 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
     const int k0 = b + lane, k1 = b + lane + 32;
     float4 f0 = f4_zero(), f1 = f4_zero(), n0 = f4_zero(), n1 = f4_zero();   // FP(x) and the neighbour
     int t0 = INT32_MAX, t1 = INT32_MAX;
+    // two 16-byte loads per record here: ptxas 12.9 fails on the 256-bit load in this function
     if (h0) { f0 = __ldg(Z + 2 * (int64_t)k0); n0 = __ldg(Z + 2 * (int64_t)k0 + 1); if (LAK) t0 = __ldg(z.T + k0); }
     if (h1) { f1 = __ldg(Z + 2 * (int64_t)k1); n1 = __ldg(Z + 2 * (int64_t)k1 + 1); if (LAK) t1 = __ldg(z.T + k1); }
     const float4 Pv = ldg4(P, v);
@@ -915,13 +1083,15 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
 // edge points of C's edges {v, e_out(x)} (ids = the slots) stream.  With a
 // boundary (BND), an edge {v, e_out(x)} without a twin gets the midpoint.
 // Columns longer than kBigCol go to their warp (g3_warp_column).
+// `nv`: the vertices of P it covers, V1 (or V2 on a GQ level, whose other
+// columns k_g1 sums).
 template <bool LAK, bool STATE, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
-                                           SlotScratch z, float* __restrict__ R, int compensated)
+                                           SlotScratch z, float* __restrict__ R, int compensated, int nv)
 {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (STATE && v == d.V1) c.sptr[d.V] = d.N;
-    const bool valid = v < d.V1;
+    if (STATE && v == nv) c.sptr[d.V] = d.N;
+    const bool valid = v < nv;
     int b = 0, n = 0;
     if (valid) { b = __ldg(p.sptr + v); n = __ldg(p.sptr + v + 1) - b; }
     const bool big = valid && n > kBigCol && n <= kWarpCol;

@@ -40,6 +40,10 @@ struct Level {
     bool fast = false;      // closed-form refinement from the parent level's state
     bool export_state = false;   // general level whose state feeds a fast level
     bool make_state = false;     // fast level whose state feeds the next fast level
+    // fast level whose parent's parent is a closed quad mesh (GQ, fast.cuh):
+    // k_g1 sums most of the parent's vertex columns; that mesh's sizes
+    bool gq = false;
+    int64_t gN = 0, gV = 0, gF = 0;
     QState in_state{}, out_state{};
     SlotScratch slots{};    // fast level: slot-ordered records from k_g1 to k_g3
     const int* ptr = nullptr;
@@ -361,10 +365,12 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
 
 // One fast level: C = L (refined from its parent level Pl, whose state is
 // L.in_state).  BND: Pl has a boundary (quad faces only).
-template <bool LAK, bool STATE, bool PQ, bool BND>
+template <bool LAK, bool STATE, bool PQ, bool BND, bool GQ = false>
 void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc& lc)
 {
     FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N, (int)Pl.B};
+    if (GQ) { d.N2 = (int)L.gN; d.V2 = (int)L.gV; d.F2 = (int)L.gF; }
+    const int nv3 = GQ ? (int)L.gV : (int)Pl.V;      // k_g3's vertices
     cudaStream_t str = lc.s;
     // compulsory bytes of each kernel: the level's corner ids and positions it
     // must read once, and the refined ids / positions it alone writes
@@ -375,11 +381,13 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g1<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, str>>>(d, pf, L.ids, L.verts, L.in_state,
-                                                                         L.out_state, reinterpret_cast<int4*>(L.o_ids),
-                                                                         L.o_verts, L.slots, optr, ovals);
+        k_g1<LAK, STATE, PQ, BS, BND, GQ><<<grid_for(L.F, BS), BS, 0, str>>>(
+            d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
+            optr, ovals);
     });
-    lc.after("k_g1", 1, (PQ ? g1b + g2b : g1b) + (optr ? 4 * (L.N + 1) + 16 * L.N : 0));
+    // GQ: k_g1 also writes the vertex points of P's vertices past V2 (and SLAK their slots' edge points)
+    const int64_t gqb = GQ ? 16 * (Pl.V - L.gV) + (LAK ? 0 : 16 * (L.F - L.gN)) : 0;
+    lc.after("k_g1", 1, (PQ ? g1b + g2b : g1b) + (optr ? 4 * (L.N + 1) + 16 * L.N : 0) + gqb);
     if (!PQ) {      // with quad faces, k_g1 also does k_gf's and k_g2's work
         // k_gf, k_g2 and k_g3 read only k_g1's records and the level's inputs and
         // write disjoint outputs: with side streams they run side by side
@@ -396,10 +404,12 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     }
     with_block(L.bs[2], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g3<LAK, STATE, BS, BND><<<grid_for(Pl.V + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
-                                                                          L.slots, L.o_verts, comp ? 1 : 0);
+        k_g3<LAK, STATE, BS, BND><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
+                                                                         L.slots, L.o_verts, comp ? 1 : 0, nv3);
     });
-    lc.after("k_g3", 1, 16 * Pl.V + (LAK ? 0 : 16 * L.F));
+    // compulsory bytes: the vertex points of its vertices, SLAK the edge points of their slots
+    const int64_t ns3 = GQ ? L.gN : L.F;
+    lc.after("k_g3", 1, 16 * (int64_t)nv3 + (LAK ? 0 : 16 * ns3));
     if (BND && STATE && !LAK) {    // C's edges 0..N1-1 (P's slots): boundary ranks by a scan
         int64_t nl = 0;
         scan_exclusive(L.slots.bscan, L.out_state.brank, Pl.N, L.scan_tmp, str, &nl);
@@ -408,15 +418,15 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     if (!PQ && lc.conc) { lc.join(0); lc.join(1); }
 }
 
-template <bool PQ, bool BND>
+template <bool PQ, bool BND, bool GQ = false>
 void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool comp, Lc& lc)
 {
     if (lak) {
-        if (L.make_state) launch_fast_t<true, true, PQ, BND>(Pl, L, pf, comp, lc);
-        else launch_fast_t<true, false, PQ, BND>(Pl, L, pf, comp, lc);
+        if (L.make_state) launch_fast_t<true, true, PQ, BND, GQ>(Pl, L, pf, comp, lc);
+        else launch_fast_t<true, false, PQ, BND, GQ>(Pl, L, pf, comp, lc);
     } else {
-        if (L.make_state) launch_fast_t<false, true, PQ, BND>(Pl, L, pf, comp, lc);
-        else launch_fast_t<false, false, PQ, BND>(Pl, L, pf, comp, lc);
+        if (L.make_state) launch_fast_t<false, true, PQ, BND, GQ>(Pl, L, pf, comp, lc);
+        else launch_fast_t<false, false, PQ, BND, GQ>(Pl, L, pf, comp, lc);
     }
 }
 
@@ -424,7 +434,8 @@ void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool
 void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, bool comp, Lc& lc)
 {
     const bool lak = scheme == SLAK_SCHEME_LAK;
-    if (Pl.quad && Pl.B > 0) launch_fast_p<true, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    if (L.gq) launch_fast_p<true, false, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else if (Pl.quad && Pl.B > 0) launch_fast_p<true, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.quad) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.B > 0) launch_fast_p<false, true>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
     else launch_fast_p<false, false>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
@@ -662,6 +673,11 @@ int plan_levels(slak_plan* p)
     }
     for (int i = 0; i < nlev; ++i) {
         Level& L = p->lv[i];
+        // GQ (on request): the parent is refine(PP) with PP a closed quad mesh
+        if (L.fast && i >= 2 && p->lv[i - 2].quad && p->lv[i - 2].B == 0 && (p->flags & SLAK_PLAN_GQ)) {
+            L.gq = true;
+            L.gN = p->lv[i - 2].N; L.gV = p->lv[i - 2].V; L.gF = p->lv[i - 2].F;
+        }
         if (L.fast && p->lv[i - 1].N > p->slN) p->slN = p->lv[i - 1].N;
         if (L.fast && p->lv[i - 1].B > 0) p->bnd_fast = true;
         if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) {
@@ -854,8 +870,8 @@ std::string tune_key(const slak_plan* p, int li)
     const int fb = (int)std::floor(std::log2((double)std::max<int64_t>(L.F, 1)));
     char buf[96];
     std::snprintf(buf, sizeof buf, "%s/%s%s/%s/q2^%d/vmax%d/v4_%d", p->scheme == SLAK_SCHEME_LAK ? "lak" : "slak",
-                  P.quad ? "quad" : "poly", P.B > 0 ? "-open" : "", L.make_state ? "state" : "last", fb, vclass,
-                  sclass);
+                  L.gq ? "gquad" : P.quad ? "quad" : "poly", P.B > 0 ? "-open" : "", L.make_state ? "state" : "last",
+                  fb, vclass, sclass);
     return buf;
 }
 
