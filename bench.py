@@ -10,6 +10,12 @@ One step = one full multi-level subdivision of that mesh.
           pinned memory, slak_subdivide, D2H of the refined ids and positions
   roofline  dominant kernel: algorithmic bytes / its CUDA-event duration
   cpu_baseline  the CPU restatement (oracle) on a bounded sample, OpenMP
+  secondary the other configurations, timed the same way: the large mesh in
+          the other scheme, the capped cylinder (7 levels, both schemes), the
+          32x32 torus and the icosphere
+  batched the 2,000-mesh batch as one CUDA graph beside the per-mesh loop of
+          plans and the per-mesh loop of slak_subdivide (--no-extras skips
+          these two blocks)
 
 --impl reference times the reference's own CUDA path (GPUPeople/SLAK compiled
 from its sources for sm_100a, oracle/_ref) on the same workload.
@@ -298,6 +304,72 @@ def run_ours(args, dist, rank, ws):
     if rank == 0 and ws == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(mesh, levels, scheme, args.cpu_budget, creases=creases)
     plan.close()
+    if ws == 1 and not args.no_extras and creases is None:
+        # the survey's other configurations, then the batched form beside the
+        # per-mesh loops (its outputs, 136 GB, need the memory the plan held)
+        out["secondary"] = secondary_configs(args, torch, stream, flush)
+        del flush
+        torch.cuda.empty_cache()
+        b = run_batch(args, torch, dist, rank, ws)
+        b.pop("clocks", None)
+        out["batched"] = b
+    return out
+
+
+def plan_time(mesh, levels, scheme, steps, warmup, stream, torch, flush):
+    """Device time of one plan execution (CUDA-graph replay, L2 flushed before
+    each step, autotuned launch shapes), with the pipeline's compulsory bytes
+    against the measured peak: the secondary configurations of the line."""
+    from slak_b200 import api
+    peak, _ = _peaks()
+    dm = api.DeviceMesh.from_host(mesh)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        plan = api.Plan(dm, levels, scheme, api._abi.PLAN_GRAPH | api._abi.PLAN_AUTOTUNE, stream=stream)
+        for _ in range(warmup):
+            plan.execute(stream)
+        plan.check(stream)
+        for i in range(steps):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            plan.execute(stream)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        plan.check(stream)
+        stats = plan.level_stats()
+        launches = plan.launches
+        plan.close()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    t = statistics.mean(ms)
+    faces = stats[-1]["out_faces"]
+    alg = sum(x["algorithmic_bytes"] for x in stats)
+    return {"refined_faces": faces, "ms_per_step": t, "value": faces / (t * 1e-3), "unit": "refined_faces/s",
+            "ms_per_step_spread": _spread(ms), "launches_per_step": launches,
+            "pipeline_roofline": {"achieved": alg / (t * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                  "frac": alg / (t * 1e-3) / 1e9 / peak, "algorithmic_bytes": alg}}
+
+
+def secondary_configs(args, torch, stream, flush):
+    """The other configurations the survey names, measured the same way as the
+    headline (device time, graph replay): the large mixed mesh under LAK, the
+    capped cylinder (valence-64 poles) at 7 levels in both schemes, and the
+    small configurations (torus 32x32 SLAK 3 levels, icosphere 4 levels)."""
+    from slak_b200 import meshgen
+    from slak_b200.mesh import LAK, SLAK
+    out = {}
+    other = "lak" if args.scheme == "slak" else "slak"
+    m, lv = _workload(args.workload)
+    if other == "lak" and m.ptr is None:
+        m = m.with_quad_ptr()
+    out[f"{args.workload}_{other}"] = plan_time(m, lv, LAK if other == "lak" else SLAK, args.steps, args.warmup,
+                                                 stream, torch, flush)
+    for name, schemes in (("cylinder", ("slak", "lak")), ("torus32", ("slak",)), ("icosphere", ("slak", "lak"))):
+        w = meshgen.workload(name)
+        for sc in schemes:
+            mm = w.mesh if sc == "slak" or w.mesh.ptr is not None else w.mesh.with_quad_ptr()
+            r = plan_time(mm, w.levels, LAK if sc == "lak" else SLAK, args.steps, args.warmup, stream, torch, flush)
+            r["config"] = f"{name}: {w.mesh.nfaces} faces, {sc.upper()}, {w.levels} levels"
+            out[f"{name}_{sc}"] = r
     return out
 
 
@@ -658,6 +730,8 @@ def main():
                     help="refine with this seeded fraction of the edges as semi-sharp creases")
     ap.add_argument("--batch-count", type=int, default=2000)
     ap.add_argument("--batch-plain-reps", type=int, default=1)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline configuration only (no secondary configurations, no batch block)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     dist, rank, ws = _dist()

@@ -211,9 +211,17 @@ enum slak_plan_flags {
     SLAK_PLAN_COMPENSATED = 4,  /* compensated (TwoSum) sums in high-valence vertex points    */
     SLAK_PLAN_TIMING = 8,       /* record a CUDA event after every launch (per-kernel times)  */
     SLAK_PLAN_AUTOTUNE = 16,    /* measure launch shapes of untuned keys at creation (below)  */
-    SLAK_PLAN_GQ = 32           /* grandparent-quad levels: k_g1 sums most of the parent's    */
+    SLAK_PLAN_GQ = 32,          /* grandparent-quad levels: k_g1 sums most of the parent's    */
                                 /* vertex columns instead of k_g3 (same results)             */
+    SLAK_PLAN_BULK_RECORDS = 64 /* closed levels: k_g3 stages its slot records in shared      */
+                                /* memory by bulk copy (TMA) (same results; see below)        */
 };
+/* SLAK_PLAN_GQ and SLAK_PLAN_BULK_RECORDS are alternative kernel layouts kept
+ * for comparison: both give the default path's results bit for bit, and both
+ * measured slower on B200, so neither is the default.  A SLAK_PLAN_BULK_RECORDS
+ * block waits on its copies at most SLAK_BULK_WAIT_POLLS mbarrier polls (read
+ * from the environment when the plan is created, default 2^20); past that it
+ * reports SLAK_ERR_TIMEOUT through slak_plan_status (0 forces that path). */
 
 typedef struct slak_kernel_timing {
     const char* name;           /* kernel name (static string)                     */

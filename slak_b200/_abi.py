@@ -16,7 +16,8 @@ SLAK_ERR_TIMEOUT, SLAK_ERR_UNSUPPORTED, SLAK_ERR_NOT_READY = 5, 6, 7
 STATUS_NAMES = {0: "SLAK_OK", 1: "SLAK_ERR_INVALID_ARG", 2: "SLAK_ERR_CUDA", 3: "SLAK_ERR_OOM",
                 4: "SLAK_ERR_BAD_MESH", 5: "SLAK_ERR_TIMEOUT", 6: "SLAK_ERR_UNSUPPORTED", 7: "SLAK_ERR_NOT_READY"}
 
-PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE, PLAN_GQ = 1, 2, 4, 8, 16, 32
+PLAN_GRAPH, PLAN_GENERAL, PLAN_COMPENSATED, PLAN_TIMING, PLAN_AUTOTUNE, PLAN_GQ, PLAN_BULK_RECORDS = (
+    1, 2, 4, 8, 16, 32, 64)
 
 # SLAK_B200_ABI_VERSION of include/slak_b200.h, which the structs and signatures here follow
 ABI_VERSION = 1

@@ -41,6 +41,12 @@
 
 namespace slak {
 
+#ifdef SLAK_FACE_SUM_SHFL
+constexpr bool kFaceSumShfl = true;       // comparison builds: the face sums by warp shuffles throughout
+#else
+constexpr bool kFaceSumShfl = false;
+#endif
+
 __device__ __forceinline__ int qnext(int x) { return (x & ~3) | ((x + 1) & 3); }
 __device__ __forceinline__ int qprev(int x) { return (x & ~3) | ((x + 3) & 3); }
 
@@ -552,11 +558,40 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
         // vertex point of P's face point V1 + (x>>2): corners 4x_j+2 of the face's quads, n = 4
         float4 nb[4], fq[4];
         int tl[4];
+        if constexpr (!LAK || BS > 256 || kFaceSumShfl) {
+            // SLAK: shuffles (measured on B200, 512x512 mixed torus: the shared
+            // memory exchange below took the last level's k_g1 from 596 to
+            // 621 us); 512-thread blocks: the staging buffer leaves no room for
+            // the exchange under the 48 KB of static shared memory
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            nb[j] = shfl4(LAK ? c1 : c3, gl | j);      // SLAK: e_in(x_j); LAK: tails e_out(x_j)
-            fq[j] = shfl4(fp, gl | j);
-            tl[j] = __shfl_sync(0xffffffffu, Q.y, gl | j);
+            for (int j = 0; j < 4; ++j) {
+                nb[j] = shfl4(LAK ? c1 : c3, gl | j);      // SLAK: e_in(x_j); LAK: tails e_out(x_j)
+                fq[j] = shfl4(fp, gl | j);
+                tl[j] = __shfl_sync(0xffffffffu, Q.y, gl | j);
+            }
+        } else {
+            // LAK: the group's values pass through shared memory.  Warp
+            // shuffles run on the L1 data pipe this kernel is bound by, one
+            // wavefront per shuffle for the whole warp, while here only the
+            // eight summing lanes (q == 0) read; LAK also ranks the tails by
+            // id.  Measured on B200 (512x512 mixed torus): last level's k_g1
+            // 769 -> 757 us.  Entry lane + lane / 4 (padded) puts the 16-byte
+            // entries those lanes read together on distinct banks.
+            __shared__ float4 xs[BS / 32][2][40];
+            __shared__ int xt[LAK ? BS / 32 : 1][40];
+            const int wv = threadIdx.x >> 5, pl = lane + (lane >> 2);
+            xs[wv][0][pl] = LAK ? c1 : c3;             // SLAK: e_in(x_j); LAK: tails e_out(x_j)
+            xs[wv][1][pl] = fp;
+            if (LAK) xt[wv][pl] = Q.y;
+            __syncwarp();
+            if (q == 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    nb[j] = xs[wv][0][pl + j];
+                    fq[j] = xs[wv][1][pl + j];
+                    tl[j] = LAK ? xt[wv][pl + j] : 0;
+                }
+            }
         }
         if (valid && q == 0) {
             float4 yv;
@@ -869,6 +904,66 @@ __device__ __forceinline__ float4 boundary_vertex(const float* __restrict__ P, c
 }
 
 // ---------------------------------------------------------------------------------------------
+// A column of n <= 4 slots from its records in registers: zf / zn the face
+// point and neighbour of each slot, tt the LAK tail id or the SLAK rotation
+// (rot - b), fl the boundary flags.  Vertex point, then (SLAK) the edge points
+// of the column's slots.
+template <bool LAK, bool STATE, bool BND>
+__device__ __forceinline__ void g3_small(const FastDims& d, const float* __restrict__ P, QState& c,
+                                         const SlotScratch& z, float* __restrict__ R, int v, int b, int n,
+                                         float4 Pv, const float4 (&zf)[4], const float4 (&zn)[4],
+                                         const int (&tt)[4], const int (&fl)[4])
+{
+    const int e = b + n;
+    const float nn = (float)(n * n);
+    float4 yv;
+    float4 acc = f4_zero();
+    if (!LAK) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) acc = f4_add(acc, zn[k]);
+        yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) yv = f4_add(yv, f4_div(zf[k], nn));
+        const int64_t EPb = (int64_t)d.V + d.N1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) {
+                if (BND && (fl[k] & 1)) {
+                    st4_cs(R, EPb + b + k, f4_mul(f4_add(Pv, zn[k]), 0.5f));
+                    continue;
+                }
+                const int r = tt[k];
+                const float4 fr = r == 0 ? zf[0] : r == 1 ? zf[1] : r == 2 ? zf[2] : zf[3];
+                const float4 half = f4_mul(f4_add(zn[k], fr), 0.25f);
+                st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), f4_mul(f4_add(Pv, zf[k]), 0.25f)), half));
+            }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) acc = f4_add(acc, zf[k]);
+        // the tails in ascending id (ids in a column are distinct)
+        int rk[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            rk[k] = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) rk[k] += (j < n && tt[j] < tt[k]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < n && rk[k] == r) acc = f4_add(acc, zn[k]);
+        yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
+    }
+    if (BND && (fl[0] | fl[1] | fl[2] | fl[3])) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
+    st_pos<STATE>(R, v, yv);
+    if (STATE) c.sptr[v] = b;
+}
+
+// ---------------------------------------------------------------------------------------------
 // One vertex of P on its own thread (columns of up to kBigCol slots, and
 // columns too long for the warp path).
 template <bool LAK, bool STATE, bool BND>
@@ -894,50 +989,7 @@ __device__ __forceinline__ void g3_vertex(FastDims d, const float* __restrict__ 
                 if (BND) fl[k] = __ldg(z.bflag + b + k);
             }
         }
-        float4 acc = f4_zero();
-        if (!LAK) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (k < n) acc = f4_add(acc, zn[k]);
-            yv = f4_add(f4_div(acc, nn), f4_div(f4_mul(Pv, (float)(n - 2)), (float)n));
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (k < n) yv = f4_add(yv, f4_div(zf[k], nn));
-            const int64_t EPb = (int64_t)d.V + d.N1;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (k < n) {
-                    if (BND && (fl[k] & 1)) {
-                        st4_cs(R, EPb + b + k, f4_mul(f4_add(Pv, zn[k]), 0.5f));
-                        continue;
-                    }
-                    const int r = tt[k];
-                    const float4 fr = r == 0 ? zf[0] : r == 1 ? zf[1] : r == 2 ? zf[2] : zf[3];
-                    const float4 half = f4_mul(f4_add(zn[k], fr), 0.25f);
-                    st4_cs(R, EPb + b + k, f4_add(f4_add(f4_zero(), f4_mul(f4_add(Pv, zf[k]), 0.25f)), half));
-                }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (k < n) acc = f4_add(acc, zf[k]);
-            // the tails in ascending id (ids in a column are distinct)
-            int rk[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                rk[k] = 0;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) rk[k] += (j < n && tt[j] < tt[k]);
-            }
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (k < n && rk[k] == r) acc = f4_add(acc, zn[k]);
-            yv = f4_div_z(f4_add(f4_div_z(acc, (float)n), f4_mul(Pv, __fadd_rn((float)n, -2.0f))), (float)n);
-        }
-        if (BND && (fl[0] | fl[1] | fl[2] | fl[3])) yv = boundary_vertex<LAK>(P, z, b, e, Pv, yv);
-        st_pos<STATE>(R, v, yv);
-        if (STATE) c.sptr[v] = b;
+        g3_small<LAK, STATE, BND>(d, P, c, z, R, v, b, n, Pv, zf, zn, tt, fl);
         return;
     }
     const bool comp = compensated && n > 4;
@@ -1102,6 +1154,103 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
         m &= m - 1;
         g3_warp_column<LAK, STATE, BND>(d, P, c, z, R, compensated, __shfl_sync(0xffffffffu, v, src),
                                         __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_g3 with its block's slot records staged in shared memory by the bulk-copy
+// (TMA) engine.  A block's vertices are consecutive, so their columns are one
+// contiguous slot range: thread 0 issues one cp.async.bulk for the range's
+// records (32 bytes a slot) and one for its rotation (SLAK) / tail (LAK)
+// indices, both completing on an mbarrier; the arithmetic is g3_small's.
+// Closed parents only (no boundary records).  Columns of more than 4 slots, and
+// blocks whose range exceeds the kBulkSlots staging buffer, read global memory
+// as k_g3 does.  The copies read this GPU's own memory, without cluster
+// multicast.  The wait is bounded: after `polls` unsuccessful polls the block
+// records SLAK_ERR_TIMEOUT, waits (again bounded) for its own copies, which
+// write its shared memory, and returns.  128-thread blocks.
+constexpr int kBulkBlock = 128;
+constexpr int kBulkSlots = 6 * kBulkBlock;
+constexpr int kBulkRetire = 1 << 22;      // polls allowed for the copies to land after a timeout
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int polls)
+{
+    for (int i = 0; i < polls; ++i) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float* __restrict__ P, QState p,
+                                                        QState c, SlotScratch z, float* __restrict__ R,
+                                                        int compensated, int nv, DevStatus* st, int polls)
+{
+    __shared__ __align__(128) float4 zs[2 * kBulkSlots];
+    __shared__ __align__(16) int rs[kBulkSlots + 8];
+    __shared__ __align__(8) unsigned long long bar;
+    const int v0 = blockIdx.x * kBulkBlock, v = v0 + threadIdx.x;
+    if (STATE && v == nv) c.sptr[d.V] = d.N;
+    if (v0 >= nv) return;                                   // the sentinel's block
+    const int vl = min(v0 + kBulkBlock, nv);
+    const int sb = __ldg(p.sptr + v0), se = __ldg(p.sptr + vl);
+    const int rb = sb & ~3, re = (se + 3) & ~3;             // 16-byte aligned index range
+    const bool staged = se - sb <= kBulkSlots;              // the same for the whole block
+    if (staged) {
+        const uint32_t sbar = (uint32_t)__cvta_generic_to_shared(&bar);
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(sbar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t zbytes = 32u * (uint32_t)(se - sb), ibytes = 4u * (uint32_t)(re - rb);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(sbar), "r"(zbytes + ibytes)
+                         : "memory");
+            if (zbytes)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             :: "r"((uint32_t)__cvta_generic_to_shared(zs)), "l"(z.Z + 2 * (int64_t)sb),
+                                "r"(zbytes), "r"(sbar) : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"((uint32_t)__cvta_generic_to_shared(rs)), "l"((LAK ? z.T : z.rot) + rb),
+                            "r"(ibytes), "r"(sbar) : "memory");
+        }
+        // the warp decides together (the column pass below shuffles across it)
+        if (!__all_sync(0xffffffffu, mbar_wait(sbar, 0, polls))) {
+            if ((threadIdx.x & 31) == 0) set_error(st, 5, 3000000 + blockIdx.x);     // SLAK_ERR_TIMEOUT
+            mbar_wait(sbar, 0, kBulkRetire);
+            return;
+        }
+    }
+    const bool valid = v < nv;
+    int b = 0, n = 0;
+    if (valid) { b = __ldg(p.sptr + v); n = __ldg(p.sptr + v + 1) - b; }
+    const bool big = valid && n > kBigCol && n <= kWarpCol;
+    if (valid && staged && n <= 4) {
+        float4 zf[4], zn[4];
+        int tt[4], fl[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < n) {
+                zf[k] = zs[2 * (b - sb + k)];
+                zn[k] = zs[2 * (b - sb + k) + 1];
+                tt[k] = LAK ? rs[b + k - rb] : rs[b + k - rb] - b;
+            }
+        g3_small<LAK, STATE, false>(d, P, c, z, R, v, b, n, ldg4(P, v), zf, zn, tt, fl);
+    } else if (valid && !big) {
+        g3_vertex<LAK, STATE, false>(d, P, c, z, R, compensated, v, b, n);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, big);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        g3_warp_column<LAK, STATE, false>(d, P, c, z, R, compensated, __shfl_sync(0xffffffffu, v, src),
+                                          __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
     }
 }
 

@@ -44,6 +44,10 @@ struct Level {
     // k_g1 sums most of the parent's vertex columns; that mesh's sizes
     bool gq = false;
     int64_t gN = 0, gV = 0, gF = 0;
+    // k_g3 with bulk-copied slot records (SLAK_PLAN_BULK_RECORDS, closed parents)
+    bool bulk3 = false;
+    int bulk_polls = 0;
+    DevStatus* st = nullptr;
     QState in_state{}, out_state{};
     SlotScratch slots{};    // fast level: slot-ordered records from k_g1 to k_g3
     const int* ptr = nullptr;
@@ -402,11 +406,16 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
         });
         lc.after("k_g2", 1, g2b);
     }
-    with_block(L.bs[2], [&](auto b) {
-        constexpr int BS = decltype(b)::value;
-        k_g3<LAK, STATE, BS, BND><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
-                                                                         L.slots, L.o_verts, comp ? 1 : 0, nv3);
-    });
+    if (!BND && L.bulk3) {
+        k_g3_bulk<LAK, STATE><<<grid_for(nv3 + 1, kBulkBlock), kBulkBlock, 0, str>>>(
+            d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
+    } else {
+        with_block(L.bs[2], [&](auto b) {
+            constexpr int BS = decltype(b)::value;
+            k_g3<LAK, STATE, BS, BND><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
+                                                                             L.slots, L.o_verts, comp ? 1 : 0, nv3);
+        });
+    }
     // compulsory bytes: the vertex points of its vertices, SLAK the edge points of their slots
     const int64_t ns3 = GQ ? L.gN : L.F;
     lc.after("k_g3", 1, 16 * (int64_t)nv3 + (LAK ? 0 : 16 * ns3));
@@ -678,6 +687,11 @@ int plan_levels(slak_plan* p)
             L.gq = true;
             L.gN = p->lv[i - 2].N; L.gV = p->lv[i - 2].V; L.gF = p->lv[i - 2].F;
         }
+        if (L.fast && p->lv[i - 1].B == 0 && (p->flags & SLAK_PLAN_BULK_RECORDS)) {
+            L.bulk3 = true;
+            const char* e = std::getenv("SLAK_BULK_WAIT_POLLS");      // tests: 0 forces the timeout path
+            L.bulk_polls = e ? std::atoi(e) : (1 << 20);
+        }
         if (L.fast && p->lv[i - 1].N > p->slN) p->slN = p->lv[i - 1].N;
         if (L.fast && p->lv[i - 1].B > 0) p->bnd_fast = true;
         if (i + 1 < nlev && p->lv[i + 1].fast && !L.fast) {
@@ -712,7 +726,7 @@ void plan_carve(slak_plan* p, Carver& cv)
     }
     if (p->slN) {
         p->slots.Z = cv.take<float4>(2 * p->slN);
-        p->slots.T = p->slots.rot = cv.take<int>(p->slN);
+        p->slots.T = p->slots.rot = cv.take<int>(p->slN + 8);     // bulk copies read whole 16-byte groups
         if (p->bnd_fast) {
             p->slots.bflag = cv.take<int>(p->slN);
             p->slots.bid = cv.take<int>(p->slN);
@@ -786,6 +800,7 @@ void plan_wire(slak_plan* p)
         if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
         L.slots = p->slots;
         L.scan_tmp = p->bnd_tmp;
+        L.st = p->st;
     }
 }
 
