@@ -104,6 +104,15 @@ __device__ __forceinline__ void ld8_nc(const float4* p, float4& a, float4& b)
         : "l"(p));
 }
 
+// Two refined quads (32 bytes, 32-byte aligned) as one 256-bit streaming
+// store: a thread's four quads are 64 contiguous bytes, two full sectors.
+__device__ __forceinline__ void st8_cs(int4* p, int4 a, int4 b)
+{
+    asm volatile("st.global.cs.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+                 :: "l"(p), "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                 : "memory");
+}
+
 // rank of corner `a` among the four corners of an edge point
 __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a) + (c < a) + (d < a); }
 
@@ -111,8 +120,7 @@ __device__ __forceinline__ int rank4(int a, int b, int c, int d) { return (b < a
 // G1: one thread per quad x of C (= corner x of P); the 4 quads of a face of P
 // are 4 consecutive lanes.  Each thread loads its quad {v, e_out, f, e_in} as
 // one int4 and the 4 corner positions, so the face point needs no exchange;
-// the block stages its 4 x 256 refined quads in shared memory and stores them
-// as one contiguous 16 KB run.
+// its 4 refined quads are 64 contiguous bytes of the output.
 // Slot-ordered records for the per-vertex pass (k_g3): for the corner x of P
 // at slot s = slot1(x), Z[2s] = FP(x) and Z[2s+1] = the position of C's next
 // (SLAK: e_out(x)) or previous (LAK: e_in(x)) vertex of corner 4x.  LAK:
@@ -419,11 +427,6 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
                                            int* __restrict__ optr, int4* __restrict__ ovals)
 {
-    // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores (consecutive
-    // t) and the run-order reads (4 k's of a t, then the next t) are both free
-    // of bank conflicts
-    constexpr int SQ = BS + 2;
-    __shared__ int4 sq[4 * SQ];
     const int x0 = blockIdx.x * blockDim.x;
     const int x = x0 + threadIdx.x;
     const bool valid = x < d.N1;
@@ -511,14 +514,30 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
         e2 = 4 * eidp_px - br_px + 2 + ((!BND || tw1_px >= 0) && fx > ftwp);
         e3 = 4 * eidp_px - br_px + (Q.x > vpx);
     }
-    // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}: staged, then one coalesced run
+    // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}.  Levels that write the
+    // next level's state: the thread's 64 bytes as two 256-bit stores.  The last
+    // level: staged in shared memory, then one coalesced run per block.
+    // Measured on B200 (512x512 mixed torus, SLAK): direct stores take level 2
+    // from 184 to 180 us and level 1 from 43 to 41 us, but the last level from
+    // 596 to 614 us.
     const int fpid = d.V + x;
-    sq[0 * SQ + threadIdx.x] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
-    sq[1 * SQ + threadIdx.x] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
-    sq[2 * SQ + threadIdx.x] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
-    sq[3 * SQ + threadIdx.x] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
-    __syncthreads();
-    {
+    if constexpr (STATE) {
+        if (valid) {
+            int4* dst = out_ids + 4 * (int64_t)x;
+            st8_cs(dst, make_int4(Q.x, VFc + e0, fpid, VFc + e3), make_int4(Q.y, VFc + e1, fpid, VFc + e0));
+            st8_cs(dst + 2, make_int4(Q.z, VFc + e2, fpid, VFc + e1), make_int4(Q.w, VFc + e3, fpid, VFc + e2));
+        }
+    } else {
+        // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores
+        // (consecutive t) and the run-order reads (4 k's of a t, then the next
+        // t) are both free of bank conflicts
+        constexpr int SQ = BS + 2;
+        __shared__ int4 sq[4 * SQ];
+        sq[0 * SQ + threadIdx.x] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
+        sq[1 * SQ + threadIdx.x] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
+        sq[2 * SQ + threadIdx.x] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
+        sq[3 * SQ + threadIdx.x] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
+        __syncthreads();
         const int nq = min(BS, d.N1 - x0);
         int4* dst = out_ids + 4 * (int64_t)x0;
 #pragma unroll
