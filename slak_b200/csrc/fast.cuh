@@ -413,6 +413,43 @@ __device__ __forceinline__ void gq_columns(const FastDims& d, QState& c, const f
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// SG: the last level with P = refine(PP), PP a closed quad mesh; `pp` is PP's
+// state, and the level before writes none.  P's twin, slot and (SLAK) t of
+// corner x = 4y + k are what write_state would have stored, from PP's twin of
+// y (of prev(y) for k = 3), PP's slot and t of y (k = 0) and, for k = 1, 3,
+// the P vertex vx at corner x (PP's edge point V2 + F2 + e, its column at
+// 2 N2 + 4e).  Branch-free: every lane loads one twin.
+template <bool LAK>
+__device__ __forceinline__ void sg_state(const FastDims& d, const QState& pp, int x, int vx, bool valid, int& tw,
+                                         int& slot, int& t)
+{
+    const int y = x >> 2, k = x & 3;
+    const int nx = qnext(y), px = qprev(y);
+    const int twl = valid ? __ldg(pp.tw + (k == 3 ? px : y)) : 0;
+    const int sl = valid && k == 0 ? __ldg(pp.slot + y) : 0;
+    const int tl = !LAK && valid && k == 0 ? __ldg(pp.t + y) : 0;
+    const int ntw = qnext(twl);
+    // the four corners of PP edge point e's column: k = 1 (e = e_out(y)) A, B, C, D;
+    // k = 3 (e = e_in(y)) A2, B2, C2, D2 (write_state)
+    const int p0 = 4 * (k == 1 ? y : px) + 1, p1 = 4 * twl + 1, p2 = k == 1 ? 4 * nx + 3 : 4 * y + 3;
+    const int p3 = 4 * ntw + 3;
+    const int r0 = rank4(p0, p1, p2, p3), r2 = rank4(p2, p0, p1, p3), r3 = rank4(p3, p0, p1, p2);
+    const int base = 2 * d.N2 + 4 * (vx - d.V2 - d.F2);
+    tw = k == 0 ? 4 * ntw + 3 : k == 1 ? 4 * nx + 2 : k == 2 ? 4 * px + 1 : 4 * twl;
+    slot = k == 0 ? sl : k == 2 ? d.N2 + y : base + (k == 1 ? r0 : r2);
+    t = k == 0 ? tl : k == 2 ? d.N2 + nx : base + (k == 1 ? r3 : r0);
+}
+
+// SG: P's column offsets from PP's (old vertices keep their columns; face
+// points at N2 + 4g, edge points at 2 N2 + 4e; v = V1 gives N1)
+__device__ __forceinline__ int sg_sptr(const FastDims& d, const int* __restrict__ ppsptr, int v)
+{
+    if (v < d.V2) return __ldg(ppsptr + v);
+    if (v < d.V2 + d.F2) return d.N2 + 4 * (v - d.V2);
+    return 2 * d.N2 + 4 * (v - d.V2 - d.F2);
+}
+
 // P's faces are quads (PQ: the 4 corners of a face are 4 consecutive lanes,
 // exchanged by shuffles) or polygons (face offsets and the corner -> face map
 // of P, `pf`; a face's corners are consecutive threads, read from memory).
@@ -421,7 +458,7 @@ __device__ __forceinline__ void gq_columns(const FastDims& d, QState& c, const f
 // optr / ovals (LAK, last level): the refined mesh's ptr[q] = 4q and
 // vals[q] = {1, 2, 3, 4}; they depend on q alone, so a block writes the 4 BS
 // refined quads of its span with consecutive threads (coalesced).
-template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false>
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
 __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c,
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
@@ -445,9 +482,13 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
     if constexpr (PQ) c3 = shfl4(c1, (threadIdx.x & 31 & ~3) | ((x + 3) & 3));
     else c3 = valid ? ldg4(P, Q.w) : f4_zero();
     int tw1x = 0, s1 = 0, t1x = 0;
-    if (valid && (LAK || STATE || PQ || BND)) tw1x = __ldg(p.tw + x);
-    if (valid) s1 = __ldg(p.slot + x);
-    if (valid && !LAK) t1x = __ldg(p.t + x);
+    if constexpr (SG) {
+        sg_state<LAK>(d, p, x, Q.x, valid, tw1x, s1, t1x);
+    } else {
+        if (valid && (LAK || STATE || PQ || BND)) tw1x = __ldg(p.tw + x);
+        if (valid) s1 = __ldg(p.slot + x);
+        if (valid && !LAK) t1x = __ldg(p.t + x);
+    }
     const int ln = gl | ((q + 1) & 3), lp = gl | ((q + 3) & 3);
     // next / previous corner of x in its face of P, and the twin of the previous one
     int nxx, px, tw1_px;
@@ -1156,7 +1197,7 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
 // Columns longer than kBigCol go to their warp (g3_warp_column).
 // `nv`: the vertices of P it covers, V1 (or V2 on a GQ level, whose other
 // columns k_g1 sums).
-template <bool LAK, bool STATE, int BS, bool BND = false>
+template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
 __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
                                            SlotScratch z, float* __restrict__ R, int compensated, int nv)
 {
@@ -1164,7 +1205,10 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
     if (STATE && v == nv) c.sptr[d.V] = d.N;
     const bool valid = v < nv;
     int b = 0, n = 0;
-    if (valid) { b = __ldg(p.sptr + v); n = __ldg(p.sptr + v + 1) - b; }
+    if (valid) {
+        if constexpr (SG) { b = sg_sptr(d, p.sptr, v); n = sg_sptr(d, p.sptr, v + 1) - b; }
+        else { b = __ldg(p.sptr + v); n = __ldg(p.sptr + v + 1) - b; }
+    }
     const bool big = valid && n > kBigCol && n <= kWarpCol;
     if (valid && !big) g3_vertex<LAK, STATE, BND>(d, P, c, z, R, compensated, v, b, n);
     unsigned m = __ballot_sync(0xffffffffu, big);

@@ -44,6 +44,10 @@ struct Level {
     // k_g1 sums most of the parent's vertex columns; that mesh's sizes
     bool gq = false;
     int64_t gN = 0, gV = 0, gF = 0;
+    // the last level, when its parent's parent is a closed quad mesh (SG,
+    // fast.cuh): it takes its parent's state in closed form from the
+    // grandparent's, so the level before writes none
+    bool sg = false;
     // k_g3 with bulk-copied slot records (SLAK_PLAN_BULK_RECORDS, closed parents)
     bool bulk3 = false;
     int bulk_polls = 0;
@@ -369,11 +373,11 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
 
 // One fast level: C = L (refined from its parent level Pl, whose state is
 // L.in_state).  BND: Pl has a boundary (quad faces only).
-template <bool LAK, bool STATE, bool PQ, bool BND, bool GQ = false>
+template <bool LAK, bool STATE, bool PQ, bool BND, bool GQ = false, bool SG = false>
 void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc& lc)
 {
     FastDims d{(int)Pl.N, (int)Pl.V, (int)Pl.F, (int)Pl.E, (int)L.V, (int)L.N, (int)Pl.B};
-    if (GQ) { d.N2 = (int)L.gN; d.V2 = (int)L.gV; d.F2 = (int)L.gF; }
+    if (GQ || SG) { d.N2 = (int)L.gN; d.V2 = (int)L.gV; d.F2 = (int)L.gF; }
     const int nv3 = GQ ? (int)L.gV : (int)Pl.V;      // k_g3's vertices
     cudaStream_t str = lc.s;
     // compulsory bytes of each kernel: the level's corner ids and positions it
@@ -385,7 +389,7 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g1<LAK, STATE, PQ, BS, BND, GQ><<<grid_for(L.F, BS), BS, 0, str>>>(
+        k_g1<LAK, STATE, PQ, BS, BND, GQ, SG><<<grid_for(L.F, BS), BS, 0, str>>>(
             d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
             optr, ovals);
     });
@@ -406,14 +410,14 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
         });
         lc.after("k_g2", 1, g2b);
     }
-    if (!BND && L.bulk3) {
+    if (!BND && !SG && L.bulk3) {
         k_g3_bulk<LAK, STATE><<<grid_for(nv3 + 1, kBulkBlock), kBulkBlock, 0, str>>>(
             d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
     } else {
         with_block(L.bs[2], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            k_g3<LAK, STATE, BS, BND><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(d, L.verts, L.in_state, L.out_state,
-                                                                             L.slots, L.o_verts, comp ? 1 : 0, nv3);
+            k_g3<LAK, STATE, BS, BND, SG><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(
+                d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3);
         });
     }
     // compulsory bytes: the vertex points of its vertices, SLAK the edge points of their slots
@@ -430,6 +434,13 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
 template <bool PQ, bool BND, bool GQ = false>
 void launch_fast_p(const Level& Pl, const Level& L, Faces<PQ> pf, bool lak, bool comp, Lc& lc)
 {
+    if constexpr (PQ && !BND) {
+        if (L.sg) {             // the last level: no state to write
+            if (lak) launch_fast_t<true, false, PQ, BND, GQ, true>(Pl, L, pf, comp, lc);
+            else launch_fast_t<false, false, PQ, BND, GQ, true>(Pl, L, pf, comp, lc);
+            return;
+        }
+    }
     if (lak) {
         if (L.make_state) launch_fast_t<true, true, PQ, BND, GQ>(Pl, L, pf, comp, lc);
         else launch_fast_t<true, false, PQ, BND, GQ>(Pl, L, pf, comp, lc);
@@ -444,6 +455,7 @@ void launch_fast(const Level& Pl, const Level& L, const int* cface, int scheme, 
 {
     const bool lak = scheme == SLAK_SCHEME_LAK;
     if (L.gq) launch_fast_p<true, false, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
+    else if (L.sg) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.quad && Pl.B > 0) launch_fast_p<true, true>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.quad) launch_fast_p<true, false>(Pl, L, Faces<true>{nullptr, nullptr}, lak, comp, lc);
     else if (Pl.B > 0) launch_fast_p<false, true>(Pl, L, Faces<false>{Pl.ptr, cface}, lak, comp, lc);
@@ -673,6 +685,14 @@ int plan_levels(slak_plan* p)
         }
         L.Fo = L.N; L.No = 4 * L.N; L.Vo = L.V + L.F + L.E;
         if (L.No >= (1ll << 31) || L.Vo >= (1ll << 31)) return SLAK_ERR_UNSUPPORTED;
+        // the parent is refine(PP) with PP a closed quad mesh: GQ on request; SG
+        // on the last level (SLAK_NO_SG builds: off, for comparisons)
+        const bool gq_parent = L.fast && i >= 2 && p->lv[i - 2].quad && p->lv[i - 2].B == 0;
+        if (gq_parent && (p->flags & SLAK_PLAN_GQ)) L.gq = true;
+#ifndef SLAK_NO_SG
+        if (gq_parent && i == nlev - 1 && p->lv[i - 1].fast) L.sg = true;
+#endif
+        if (L.gq || L.sg) { L.gN = p->lv[i - 2].N; L.gV = p->lv[i - 2].V; L.gF = p->lv[i - 2].F; }
         if (!L.fast) {
             if (L.N > p->maxN) p->maxN = L.N;
             if (L.V > p->maxV) p->maxV = L.V;
@@ -682,11 +702,6 @@ int plan_levels(slak_plan* p)
     }
     for (int i = 0; i < nlev; ++i) {
         Level& L = p->lv[i];
-        // GQ (on request): the parent is refine(PP) with PP a closed quad mesh
-        if (L.fast && i >= 2 && p->lv[i - 2].quad && p->lv[i - 2].B == 0 && (p->flags & SLAK_PLAN_GQ)) {
-            L.gq = true;
-            L.gN = p->lv[i - 2].N; L.gV = p->lv[i - 2].V; L.gF = p->lv[i - 2].F;
-        }
         if (L.fast && p->lv[i - 1].B == 0 && (p->flags & SLAK_PLAN_BULK_RECORDS)) {
             L.bulk3 = true;
             const char* e = std::getenv("SLAK_BULK_WAIT_POLLS");      // tests: 0 forces the timeout path
@@ -699,7 +714,7 @@ int plan_levels(slak_plan* p)
             if (L.N > p->exN) p->exN = L.N;
             if (L.B > 0 && L.E > p->exE) p->exE = L.E;
         }
-        if (L.fast && i + 1 < nlev && p->lv[i + 1].fast) {
+        if (L.fast && i + 1 < nlev && p->lv[i + 1].fast && !p->lv[i + 1].sg) {
             L.make_state = true;
             if (L.N > p->stN) p->stN = L.N;
             if (L.V > p->stV) p->stV = L.V;
@@ -795,7 +810,8 @@ void plan_wire(slak_plan* p)
         Level& L = p->lv[i];
         if (!L.fast) continue;
         const Level& P = p->lv[i - 1];
-        if (P.export_state) L.in_state = QState{p->s.sptr, p->s.xslot, p->s.xtw, p->s.xt, p->s.xbrank};
+        if (L.sg) L.in_state = P.in_state;      // the grandparent's state: the parent's own input
+        else if (P.export_state) L.in_state = QState{p->s.sptr, p->s.xslot, p->s.xtw, p->s.xt, p->s.xbrank};
         else L.in_state = P.out_state;
         if (L.make_state) { L.out_state = p->qs[qi]; qi ^= 1; }
         L.slots = p->slots;
@@ -885,7 +901,8 @@ std::string tune_key(const slak_plan* p, int li)
     const int fb = (int)std::floor(std::log2((double)std::max<int64_t>(L.F, 1)));
     char buf[96];
     std::snprintf(buf, sizeof buf, "%s/%s%s/%s/q2^%d/vmax%d/v4_%d", p->scheme == SLAK_SCHEME_LAK ? "lak" : "slak",
-                  L.gq ? "gquad" : P.quad ? "quad" : "poly", P.B > 0 ? "-open" : "", L.make_state ? "state" : "last",
+                  L.gq ? "gquad" : P.quad ? "quad" : "poly", P.B > 0 ? "-open" : "",
+                  L.make_state ? "state" : L.sg ? "last-sg" : "last",
                   fb, vclass, sclass);
     return buf;
 }

@@ -176,3 +176,49 @@ def test_grandparent_quad_columns(name, make, scheme):
         vp = _vp_lak(Pv, [tl[:, k] for k in range(4)], [tid[:, k] for k in range(4)],
                      [take(fq, r) for r in range(4)])
     assert np.array_equal(vp.view(np.uint32), R[v].view(np.uint32))
+
+
+@pytest.mark.parametrize("scheme", [SLAK, LAK])
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_parent_state_from_grandparent(name, make, scheme):
+    """The last level's parent state in closed form (k_g1 / k_g3 with SG):
+    P = refine(PP), PP a closed quad mesh.  P corner x = 4y + k takes its twin,
+    slot and (SLAK) t from PP's twin / slot / t at y and prev(y) and from the
+    P vertex at corner x itself (for k = 1, 3 an edge point V2 + F2 + e); P's
+    column offsets come from PP's for PP's old vertices and in closed form for
+    face points (N2 + 4g) and edge points (2 N2 + 4e)."""
+    base = make()
+    if scheme == LAK and base.ptr is None:
+        base = base.with_quad_ptr()
+    PP = _closed_quad(base, scheme)
+    Pr = oracle.level(PP if scheme == SLAK else PP.with_quad_ptr(), scheme, poly=False)
+    N2, V2 = PP.nnz, PP.nverts
+    F2 = N2 // 4
+    stPP = brute_state(PP.ids, V2, scheme)
+    stP = brute_state(Pr.ids, Pr.nverts, scheme)
+    idsP = Pr.ids.astype(np.int64)
+    x = np.arange(Pr.nnz)
+    y, k = x >> 2, x & 3
+    nx, px = qn(y), qp(y)
+    tw2, tw2p = stPP["tw"][y], stPP["tw"][px]
+    ntw, ntwp = qn(tw2), qn(tw2p)
+    eidp = idsP[x] - V2 - F2                              # k = 1: e_out(y); k = 3: e_in(y)
+    rk = lambda a, b, c, d: (b < a).astype(np.int64) + (c < a) + (d < a)
+    A, B, Cc, D = 4 * y + 1, 4 * tw2 + 1, 4 * nx + 3, 4 * ntw + 3
+    A2, B2, C2, D2 = 4 * px + 1, 4 * tw2p + 1, 4 * y + 3, 4 * ntwp + 3
+    base_ = 2 * N2 + 4 * eidp
+    tw = np.select([k == 0, k == 1, k == 2], [4 * ntw + 3, 4 * nx + 2, 4 * px + 1], 4 * tw2p)
+    slot = np.select([k == 0, k == 1, k == 2], [stPP["slot"][y], base_ + rk(A, B, Cc, D), N2 + y],
+                     base_ + rk(C2, A2, B2, D2))
+    assert np.array_equal(tw, stP["tw"])
+    assert np.array_equal(slot, stP["slot"])
+    if scheme == SLAK:
+        t = np.select([k == 0, k == 1, k == 2], [stPP["t"][y], base_ + rk(D, A, B, Cc), N2 + nx],
+                      base_ + rk(A2, B2, C2, D2))
+        assert np.array_equal(t, stP["t"])
+    v = np.arange(Pr.nverts + 1)
+    E2 = N2 // 2
+    sptr = np.where(v < V2, stPP["sptr"][np.minimum(v, V2)],
+                    np.where(v < V2 + F2, N2 + 4 * (v - V2), 2 * N2 + 4 * (v - V2 - F2)))
+    assert np.array_equal(sptr, stP["sptr"])
+    assert sptr[-1] == 4 * N2 and Pr.nverts == V2 + F2 + E2

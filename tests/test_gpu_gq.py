@@ -67,3 +67,6 @@ def test_gq_level_kinds_in_the_tuning_key():
     p.close()
     assert "gquad" not in keys[0] and "gquad" not in keys[1]      # levels 1, 2: polygon grandparent
     assert "/gquad/" in keys[2]                                     # level 3: PP = level 1's quads
+    # the last level takes its parent's state from the grandparent's (SG), so
+    # level 2 writes none
+    assert "/state/" in keys[0] and "/last/" in keys[1] and "/last-sg/" in keys[2]
