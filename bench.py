@@ -41,10 +41,11 @@ sys.path.insert(0, HERE)
 HBM_FALLBACK_GBS = 6650.0
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per unit of work of a
-# kernel, from one ncu capture of a smaller case of the same structure
-# (profiles/k_g_fast_levels_mixed384_slak.txt: k_g1 of the last level, SLAK,
-# per quad of the level it refines); scaled by the units of the bench's launch.
-TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 183.03}
+# kernel, from one single-pass ncu capture of the bench workload itself
+# (profiles/k_g1_k_g3_last_level_mixed512_slak.txt: k_g1 of the last level,
+# SLAK, per quad of the level it refines, this build); times the units of the
+# bench's launch.
+TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 174.53}
 # B200 HBM3e datasheet bandwidth (DGX figure), reported beside the measured peak
 HBM_NOMINAL_GBS = 8000.0
 
@@ -264,7 +265,7 @@ def run_ours(args, dist, rank, ws):
     if tpu is not None:
         units = stats[kern["level"]]["nfaces"]
         kern["traffic"] = tpu * units
-        kern["traffic_note"] = (f"{tpu} B per quad refined (ncu, mixed:384 capture) x {units} quads; "
+        kern["traffic_note"] = (f"{tpu} B per quad refined (ncu, one pass, mixed512 capture) x {units} quads; "
                                 f"{tpu * units / kern['algorithmic_bytes_per_launch']:.2f}x the algorithmic bytes")
 
     # ms per level: the per-kernel event times summed by level, with the level's
