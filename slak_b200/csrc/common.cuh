@@ -7,11 +7,49 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace slak {
 
 constexpr int kBlock = 256;
+
+// ------------------------------------------------------- dependent launches
+// Programmatic dependent launch: every kernel is launched with the
+// programmatic-serialization attribute and starts with griddep_enter(): it
+// waits until the grid before it in the stream has completed and its memory
+// is visible (griddepcontrol.wait returns at once when there is none), then
+// allows the grid after it to begin launching.  So each launch overlaps the
+// tail of the grid before it instead of following its end, while no thread
+// touches memory before its predecessor is done.  SLAK_NO_PDL builds launch
+// plainly, for comparisons.
+__device__ __forceinline__ void griddep_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+#ifdef SLAK_NO_PDL
+constexpr bool kUsePdl = false;
+#else
+constexpr bool kUsePdl = true;
+#endif
+
+template <class... KArgs, class... Args>
+inline void launch_k(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = kUsePdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // ---------------------------------------------------------------- float4 ops
 __device__ __forceinline__ float4 f4_add(float4 a, float4 b)

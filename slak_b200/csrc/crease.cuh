@@ -65,6 +65,7 @@ __global__ void k_crease_resolve(const int* __restrict__ pairs, const float* __r
                                  const int* __restrict__ snext, int* __restrict__ mark, int* __restrict__ cc,
                                  float* __restrict__ cs, DevStatus* st)
 {
+    griddep_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     const int a = __ldg(pairs + 2 * i), b = __ldg(pairs + 2 * i + 1);
@@ -95,6 +96,7 @@ __global__ void k_crease_vinc(int V, const int* __restrict__ sptr, const int* __
                               const int* __restrict__ mark, int* __restrict__ vcnt, unsigned char* __restrict__ bnd0,
                               const int* __restrict__ vptr, int* __restrict__ inc)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     int k = 0, f = 0;
@@ -120,6 +122,7 @@ __global__ void k_crease_edges(Faces<QUAD> fc, const int* __restrict__ ids, cons
                                const float* __restrict__ cs, int n, int* __restrict__ ncc, float* __restrict__ ncs,
                                int* __restrict__ epid)
 {
+    griddep_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int c = cc[i];
@@ -171,6 +174,7 @@ __global__ void k_crease_verts(Faces<QUAD> fc, int l, int V0, int64_t m, const i
                                const int* __restrict__ inc, const unsigned char* __restrict__ bnd0, CreaseEps eps,
                                const float* __restrict__ vcs, const float* __restrict__ P, float* __restrict__ R)
 {
+    griddep_enter();
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < V0) {
         const int v = (int)idx;

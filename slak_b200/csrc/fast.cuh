@@ -431,10 +431,16 @@ __device__ __forceinline__ void sg_state(const FastDims& d, const QState& pp, in
     const int tl = !LAK && valid && k == 0 ? __ldg(pp.t + y) : 0;
     const int ntw = qnext(twl);
     // the four corners of PP edge point e's column: k = 1 (e = e_out(y)) A, B, C, D;
-    // k = 3 (e = e_in(y)) A2, B2, C2, D2 (write_state)
-    const int p0 = 4 * (k == 1 ? y : px) + 1, p1 = 4 * twl + 1, p2 = k == 1 ? 4 * nx + 3 : 4 * y + 3;
-    const int p3 = 4 * ntw + 3;
-    const int r0 = rank4(p0, p1, p2, p3), r2 = rank4(p2, p0, p1, p3), r3 = rank4(p3, p0, p1, p2);
+    // k = 3 (e = e_in(y)) A2, B2, C2, D2 (write_state).  Two of them, p0 and
+    // p2, lie in y's PP face (P corners 16 face(y) .. +15), the other two, p1
+    // and p3, in the twin's, so their ranks follow from the faces' order and
+    // the order within each pair: p0 > p2 when y is corner 3 (k = 1) or
+    // corner 0 (k = 3) of its face, p1 > p3 when the twin is corner 3 of its.
+    const bool own_first = (y >> 2) < (twl >> 2);
+    const int o = own_first ? 0 : 2;
+    const int r0 = o + ((y & 3) == (k == 1 ? 3 : 0));
+    const int r2 = o + ((y & 3) != (k == 1 ? 3 : 0));
+    const int r3 = (2 - o) + ((twl & 3) != 3);
     const int base = 2 * d.N2 + 4 * (vx - d.V2 - d.F2);
     tw = k == 0 ? 4 * ntw + 3 : k == 1 ? 4 * nx + 2 : k == 2 ? 4 * px + 1 : 4 * twl;
     slot = k == 0 ? sl : k == 2 ? d.N2 + y : base + (k == 1 ? r0 : r2);
@@ -464,6 +470,7 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
                                            int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
                                            int* __restrict__ optr, int4* __restrict__ ovals)
 {
+    griddep_enter();
     const int x0 = blockIdx.x * blockDim.x;
     const int x = x0 + threadIdx.x;
     const bool valid = x < d.N1;
@@ -556,11 +563,12 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
         e3 = 4 * eidp_px - br_px + (Q.x > vpx);
     }
     // refined quads {v_k, V+F+e_k, V+x, V+F+e_(k-1)}.  Levels that write the
-    // next level's state: the thread's 64 bytes as two 256-bit stores.  The last
-    // level: staged in shared memory, then one coalesced run per block.
-    // Measured on B200 (512x512 mixed torus, SLAK): direct stores take level 2
-    // from 184 to 180 us and level 1 from 43 to 41 us, but the last level from
-    // 596 to 614 us.
+    // next level's state: the thread's 64 bytes as two 256-bit stores.  Other
+    // levels: staged in shared memory, then one coalesced run per block.
+    // Measured on B200 (512x512 mixed torus, SLAK): direct stores take a
+    // state-writing level 2 from 184 to 180 us and level 1 from 43 to 41 us,
+    // but the last level from 596 to 614 us (and a level 2 without state, as SG
+    // makes it, from 154 to 166 us).
     const int fpid = d.V + x;
     if constexpr (STATE) {
         if (valid) {
@@ -778,6 +786,7 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
                                                const float* __restrict__ P, QState c, float* __restrict__ R,
                                                int compensated)
 {
+    griddep_enter();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= d.F1) return;
     const int b = __ldg(pptr + g), e = __ldg(pptr + g + 1), k = e - b;
@@ -884,6 +893,7 @@ template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                            const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
 {
+    griddep_enter();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = x < d.N1;
     const int lane = threadIdx.x & 31, q = x & 3;
@@ -1201,6 +1211,7 @@ template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
 __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
                                            SlotScratch z, float* __restrict__ R, int compensated, int nv)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (STATE && v == nv) c.sptr[d.V] = d.N;
     const bool valid = v < nv;
@@ -1253,6 +1264,7 @@ __global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float*
                                                         QState c, SlotScratch z, float* __restrict__ R,
                                                         int compensated, int nv, DevStatus* st, int polls)
 {
+    griddep_enter();
     __shared__ __align__(128) float4 zs[2 * kBulkSlots];
     __shared__ __align__(16) int rs[kBulkSlots + 8];
     __shared__ __align__(8) unsigned long long bar;
@@ -1322,6 +1334,7 @@ __global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float*
 // the scan that gives the edges' boundary ranks to the first fast level
 __global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restrict__ isb)
 {
+    griddep_enter();
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
     const int2 h = H[e];

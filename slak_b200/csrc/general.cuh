@@ -34,6 +34,7 @@ enum : int { SF_OWNER = 1, SF_BOUT = 2, SF_BIN = 4 };
 __global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
                                    int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
 {
+    griddep_enter();
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f == 0 && (ptr[0] != 0 || ptr[F] != N)) set_error(st, 4, -1);
     if (f >= F) return;
@@ -49,6 +50,7 @@ __global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __res
 
 __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
 {
+    griddep_enter();
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     int v = ids[c];
@@ -60,6 +62,7 @@ __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __rest
 // level-0 probe
 __global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restrict__ hist)
 {
+    griddep_enter();
     __shared__ int h[17];
     if (threadIdx.x < 17) h[threadIdx.x] = 0;
     __syncthreads();
@@ -77,6 +80,7 @@ __global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restr
 __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
                          int* __restrict__ fill, int* __restrict__ loose)
 {
+    griddep_enter();
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     int v = ids[c];
@@ -106,6 +110,7 @@ __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, cons
                         const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
                         int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int b = 0, n = 0;
@@ -206,6 +211,7 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
                         const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
                         int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int nb = 0, b = 0, n = 0;
@@ -277,6 +283,7 @@ __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __re
                             const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
                             int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
 {
+    griddep_enter();
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
     if (v >= V) return;
@@ -401,6 +408,7 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
                            int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
                            int li)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
     const bool valid = v < V;
@@ -426,6 +434,7 @@ __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int*
                          int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
                          int* __restrict__ xt)
 {
+    griddep_enter();
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= N) return;
     const int VF = V + F;
@@ -450,6 +459,7 @@ __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int*
 __global__ void k_fp_slak_quad(const int4* __restrict__ ids4, const float* __restrict__ P, int F,
                                float* __restrict__ FP)
 {
+    griddep_enter();
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F) return;
     int4 q = __ldg(ids4 + f);
@@ -465,6 +475,7 @@ template <bool QUAD, bool LAK>
 __global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
                          int F, float* __restrict__ FP)
 {
+    griddep_enter();
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F) return;
     int b = QUAD ? 4 * f : ptr[f], e = QUAD ? 4 * f + 4 : ptr[f + 1];
@@ -483,6 +494,7 @@ template <bool QUAD, bool LAK>
 __global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
                      const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
 {
+    griddep_enter();
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
     int2 h = __ldg(H + e);
@@ -599,6 +611,7 @@ __global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, c
                           const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
                           const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = v < V;
     int b = 0, n = 0;
@@ -755,6 +768,7 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
                          const int* __restrict__ eid, int boundary, const float* __restrict__ P,
                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
+    griddep_enter();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = v < V;
     int b = 0, n = 0;

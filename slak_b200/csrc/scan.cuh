@@ -48,6 +48,7 @@ __device__ __forceinline__ int block_excl_scan(int x, int* total)
 
 __global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ tsum)
 {
+    griddep_enter();
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
     int s = 0;
 #pragma unroll
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ 
 // one block: exclusive scan of the tile sums in place, tsum[nt] = grand total
 __global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, int nt)
 {
+    griddep_enter();
     __shared__ int tot;
     int carry = 0;
     for (int base = 0; base < nt; base += kBlock) {
@@ -81,6 +83,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, i
 __global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ in, int64_t n,
                                                        const int* __restrict__ tsum, int nt, int* __restrict__ out)
 {
+    griddep_enter();
     __shared__ int tile[kScanTile];
     __shared__ int tot;
     const int64_t base = (int64_t)blockIdx.x * kScanTile;
@@ -116,6 +119,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restri
                                                              const int* __restrict__ tsum, int nt,
                                                              int* __restrict__ out)
 {
+    griddep_enter();
     __shared__ int tile[kScanTile];
     __shared__ int tot;
     int before = 0, all = 0;
@@ -163,14 +167,14 @@ inline void scan_exclusive(const int* in, int* out, int64_t n, int* tmp, cudaStr
 {
     int64_t nt = scan_tiles(n);
     if (nt < 1) nt = 1;
-    k_scan_reduce<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp);
+    launch_k(k_scan_reduce, (unsigned)nt, kBlock, s, in, n, tmp);
     if (nt <= kScanSmallTiles) {
-        k_scan_final_small<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp, (int)nt, out);
+        launch_k(k_scan_final_small, (unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
         if (launches) *launches += 2;
         return;
     }
-    k_scan_tiles<<<1, kBlock, 0, s>>>(tmp, (int)nt);
-    k_scan_final<<<(unsigned)nt, kBlock, 0, s>>>(in, n, tmp, (int)nt, out);
+    launch_k(k_scan_tiles, 1, kBlock, s, tmp, (int)nt);
+    launch_k(k_scan_final, (unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
     if (launches) *launches += 3;
 }
 

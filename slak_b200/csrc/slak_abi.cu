@@ -273,17 +273,17 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
     if (!L.quad) {
         cudaMemsetAsync(s.cface, 0, sizeof(int) * (size_t)N, str);
-        k_face_map_valence<<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, F, N, V, s.cface, s.cnt, st);
+        launch_k(k_face_map_valence, grid_for(F), kBlock, str, L.ptr, L.ids, F, N, V, s.cface, s.cnt, st);
         lc.after("k_face_map_valence");
     } else {
-        k_valence<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.cnt, st);
+        launch_k(k_valence, grid_for(N), kBlock, str, L.ids, N, V, s.cnt, st);
         lc.after("k_valence");
     }
     int64_t dummy = 0;
     scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, &dummy);
     lc.after("scan(valence)", 3);
     // the unsorted columns live in sflag until k_edges writes the flags
-    k_bucket<<<grid_for(N), kBlock, 0, str>>>(L.ids, N, V, s.sptr, s.cnt, s.sflag);
+    launch_k(k_bucket, grid_for(N), kBlock, str, L.ids, N, V, s.sptr, s.cnt, s.sflag);
     lc.after("k_bucket");
     int* bcount = &st->bcount[li];
     // a general quad level feeding the fast path exports corner -> slot / twin
@@ -291,19 +291,19 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     int* xtw = L.export_state ? s.xtw : nullptr;
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
-        k_vsort<true><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_k(k_vsort<true>, grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                                        s.sprevc, xslot);
     } else {
         Faces<false> fc{L.ptr, s.cface};
-        k_vsort<false><<<grid_for(V), kBlock, 0, str>>>(fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_k(k_vsort<false>, grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                                         s.sprevc, xslot);
     }
     lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
-        k_edges<true><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+        launch_k(k_edges<true>, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
                                                         s.sflag, s.ecnt, bcount, xtw, st);
     else
-        k_edges<false><<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+        launch_k(k_edges<false>, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
                                                          s.sflag, s.ecnt, bcount, xtw, st);
     lc.after("k_edges");
     scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, &dummy);
@@ -323,10 +323,10 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     Faces<QUAD> fc{L.ptr, s.cface};
     const int* bcount = &st->bcount[li];
     if (lak)
-        k_eids_lak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
+        launch_k(k_eids_lak, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
                                                      s.H, st, bcount, (int)L.B, li);
     else
-        k_eids_slak<<<grid_for(V), kBlock, 0, str>>>(V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
+        launch_k(k_eids_slak, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
                                                       bcount, (int)L.B, li);
     lc.after("k_eids");
     // the refined quads (side stream 0) need only the edge ids; the positions
@@ -334,12 +334,12 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     if (lc.conc) lc.fork(0);
     cudaStream_t s_ref = lc.conc ? lc.side[0] : str;
     if (lak)
-        k_refine<QUAD, true><<<grid_for(N), kBlock, 0, s_ref>>>(fc, L.ids, s.eid, N, V, F,
+        launch_k(k_refine<QUAD, true>, grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
                                                                 reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
                                                                 reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
                                                                 nullptr);
     else
-        k_refine<QUAD, false><<<grid_for(N), kBlock, 0, s_ref>>>(fc, L.ids, s.eid, N, V, F,
+        launch_k(k_refine<QUAD, false>, grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
                                                                  reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
                                                                  s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
     lc.after("k_refine");
@@ -347,25 +347,25 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     float* FPo = R + 4 * (size_t)V;
     float* EPo = R + 4 * ((size_t)V + (size_t)F);
     if (!lak && QUAD && !L.poly_fn)
-        k_fp_slak_quad<<<grid_for(F), kBlock, 0, str>>>(reinterpret_cast<const int4*>(L.ids), L.verts, F, FPo);
+        launch_k(k_fp_slak_quad, grid_for(F), kBlock, str, reinterpret_cast<const int4*>(L.ids), L.verts, F, FPo);
     else if (lak)
-        k_fp_seq<QUAD, true><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
+        launch_k(k_fp_seq<QUAD, true>, grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
     else
-        k_fp_seq<QUAD, false><<<grid_for(F), kBlock, 0, str>>>(L.ptr, L.ids, L.verts, F, FPo);
+        launch_k(k_fp_seq<QUAD, false>, grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
     lc.after("k_fp");
     if (lc.conc) lc.fork(1);
     cudaStream_t s_ep = lc.conc ? lc.side[1] : str;
     if (lak)
-        k_ep<QUAD, true><<<grid_for(E), kBlock, 0, s_ep>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        launch_k(k_ep<QUAD, true>, grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
     else
-        k_ep<QUAD, false><<<grid_for(E), kBlock, 0, s_ep>>>(fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        launch_k(k_ep<QUAD, false>, grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
     lc.after("k_ep");
     const int bnd = L.B > 0;
     if (lak)
-        k_vp_lak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
+        launch_k(k_vp_lak<QUAD>, grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
                                                         s.eid, bnd, L.verts, FPo, R, compensated);
     else
-        k_vp_slak<QUAD><<<grid_for(V), kBlock, 0, str>>>(fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
+        launch_k(k_vp_slak<QUAD>, grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
                                                          L.verts, FPo, R, compensated);
     lc.after("k_vp");
     if (lc.conc) { lc.join(0); lc.join(1); }
@@ -389,8 +389,7 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        k_g1<LAK, STATE, PQ, BS, BND, GQ, SG><<<grid_for(L.F, BS), BS, 0, str>>>(
-            d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
+        launch_k(k_g1<LAK, STATE, PQ, BS, BND, GQ, SG>, grid_for(L.F, BS), BS, str, d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
             optr, ovals);
     });
     // GQ: k_g1 also writes the vertex points of P's vertices past V2 (and SLAK their slots' edge points)
@@ -400,24 +399,20 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
         // k_gf, k_g2 and k_g3 read only k_g1's records and the level's inputs and
         // write disjoint outputs: with side streams they run side by side
         if (lc.conc) { lc.fork(0); lc.fork(1); }
-        k_gf<LAK, STATE><<<grid_for(Pl.F), kBlock, 0, lc.conc ? lc.side[0] : str>>>(
-            d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts, comp ? 1 : 0);
+        launch_k(k_gf<LAK, STATE>, grid_for(Pl.F), kBlock, lc.conc ? lc.side[0] : str, d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts, comp ? 1 : 0);
         lc.after("k_gf");
         with_block(L.bs[1], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            k_g2<LAK, STATE, PQ, BS, BND><<<grid_for(L.F, BS), BS, 0, lc.conc ? lc.side[1] : str>>>(
-                d, pf, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+            launch_k(k_g2<LAK, STATE, PQ, BS, BND>, grid_for(L.F, BS), BS, lc.conc ? lc.side[1] : str, d, pf, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
         });
         lc.after("k_g2", 1, g2b);
     }
     if (!BND && !SG && L.bulk3) {
-        k_g3_bulk<LAK, STATE><<<grid_for(nv3 + 1, kBulkBlock), kBulkBlock, 0, str>>>(
-            d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
+        launch_k(k_g3_bulk<LAK, STATE>, grid_for(nv3 + 1, kBulkBlock), kBulkBlock, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
     } else {
         with_block(L.bs[2], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            k_g3<LAK, STATE, BS, BND, SG><<<grid_for(nv3 + 1, BS), BS, 0, str>>>(
-                d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3);
+            launch_k(k_g3<LAK, STATE, BS, BND, SG>, grid_for(nv3 + 1, BS), BS, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3);
         });
     }
     // compulsory bytes: the vertex points of its vertices, SLAK the edge points of their slots
@@ -475,23 +470,23 @@ void launch_creases_t(slak_plan* p, int li, Faces<QUAD> fc, Lc& lc)
     const int V0 = (int)L0.V;
     if (li == 0) {
         cudaMemsetAsync(p->c_mark, 0, sizeof(int) * (size_t)L0.N, str);
-        k_crease_resolve<<<grid_for(m), kBlock, 0, str>>>(p->c_pairs, p->c_sharp, (int)m, V0, p->s.sptr, p->s.sc,
+        launch_k(k_crease_resolve, grid_for(m), kBlock, str, p->c_pairs, p->c_sharp, (int)m, V0, p->s.sptr, p->s.sc,
                                                           p->s.snext, p->c_mark, p->c_cc[0], p->c_cs[0], p->st);
         lc.after("k_crease_resolve");
-        k_crease_vinc<false><<<grid_for(V0), kBlock, 0, str>>>(V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
+        launch_k(k_crease_vinc<false>, grid_for(V0), kBlock, str, V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
                                                                SF_BOUT | SF_BIN, p->c_mark, p->c_vcnt, p->c_bnd0,
                                                                nullptr, nullptr);
         lc.after("k_crease_vinc");
         int64_t ns = 0;
         scan_exclusive(p->c_vcnt, p->c_vptr, V0, p->s.tmp, str, &ns);
         lc.after("scan(crease vertices)", (int)ns);
-        k_crease_vinc<true><<<grid_for(V0), kBlock, 0, str>>>(V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
+        launch_k(k_crease_vinc<true>, grid_for(V0), kBlock, str, V0, p->s.sptr, p->s.sc, p->s.sprevc, p->s.sflag,
                                                               SF_BOUT | SF_BIN, p->c_mark, nullptr, nullptr,
                                                               p->c_vptr, p->c_inc);
         lc.after("k_crease_vinc");
     }
     const bool more = li + 1 < p->crease_levels;
-    k_crease_edges<QUAD><<<grid_for(n), kBlock, 0, str>>>(fc, L.ids, L.o_ids, L.verts, L.o_verts, p->c_cc[li],
+    launch_k(k_crease_edges<QUAD>, grid_for(n), kBlock, str, fc, L.ids, L.o_ids, L.verts, L.o_verts, p->c_cc[li],
                                                           p->c_cs[li], (int)n, more ? p->c_cc[li + 1] : nullptr,
                                                           more ? p->c_cs[li + 1] : nullptr,
                                                           more ? p->c_ep[li] : nullptr);
@@ -499,7 +494,7 @@ void launch_creases_t(slak_plan* p, int li, Faces<QUAD> fc, Lc& lc)
     CreaseEps eps{};
     for (int t = 0; t < li; ++t) eps.epid[t] = p->c_ep[t];
     const int64_t nv = (int64_t)V0 + m * ((1ll << li) - 1);
-    k_crease_verts<QUAD><<<grid_for(nv), kBlock, 0, str>>>(fc, li, V0, m, L.ids, p->c_cc[li], p->c_cs[li],
+    launch_k(k_crease_verts<QUAD>, grid_for(nv), kBlock, str, fc, li, V0, m, L.ids, p->c_cc[li], p->c_cs[li],
                                                            p->c_vcnt, p->c_vptr, p->c_inc, p->c_bnd0, eps, p->c_vcs, L.verts,
                                                            L.o_verts);
     lc.after("k_crease_verts");
@@ -546,7 +541,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         if (L.quad) launch_rest<true>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
         else launch_rest<false>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
         if (L.export_state && L.B > 0) {     // the edges' boundary ranks
-            k_export_bflag<<<grid_for(L.E), kBlock, 0, str>>>((int)L.E, p->s.H, p->s.xisb);
+            launch_k(k_export_bflag, grid_for(L.E), kBlock, str, (int)L.E, p->s.H, p->s.xisb);
             lc.after("k_export_bflag");
             int64_t n3 = 0;
             scan_exclusive(p->s.xisb, p->s.xbrank, L.E, p->s.tmp, str, &n3);
@@ -615,7 +610,7 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str, void* given = nullpt
     Lc lc{str, &nl, p->debug, 0};
     cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
     launch_topology_a(L0, 0, p->scheme, s, st, lc);
-    k_valence_hist<<<grid_for(L0.V), kBlock, 0, str>>>((int)L0.V, s.sptr, st->vhist);
+    launch_k(k_valence_hist, grid_for(L0.V), kBlock, str, (int)L0.V, s.sptr, st->vhist);
     cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
@@ -1549,7 +1544,7 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
                 if (!p) continue;
                 cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
                 launch_topology_a(p->lv[0], 0, scheme, sc, st, lc);
-                k_valence_hist<<<grid_for(p->lv[0].V), kBlock, 0, str>>>((int)p->lv[0].V, sc.sptr, st->vhist);
+                launch_k(k_valence_hist, grid_for(p->lv[0].V), kBlock, str, (int)p->lv[0].V, sc.sptr, st->vhist);
                 cudaMemcpyAsync(&b->h_st[i], st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
                 cudaMemcpyAsync(&b->h_st[i].nedges, sc.eptr + p->lv[0].V, sizeof(int), cudaMemcpyDeviceToHost, str);
             }
