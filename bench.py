@@ -582,7 +582,7 @@ def run_batch(args, torch, dist, rank, ws):
            "speedup": plain_ms / batch_ms, "unit": "refined_faces/s",
            "plan_loop_ms": plan_ms, "plan_loop_value": faces * ws / (plan_ms * 1e-3),
            "speedup_vs_plan_loop": plan_ms / batch_ms,
-           "waves": b.waves, "launches_per_execution": b.launches,
+           "waves": b.waves, "groups": b.groups, "launches_per_execution": b.launches,
            "create_s": create_s, "generate_s": gen_s, "clocks": clk.summary(),
            "plain": "slak_subdivide per mesh (allocates and frees its output per call)",
            "plan_loop": "per mesh: plan created untimed, one eager execution timed with CUDA events",

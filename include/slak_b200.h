@@ -338,10 +338,22 @@ int slak_subdivide_sharp(const slak_mesh* cmesh, slak_mesh* rmesh, int target_le
  * source/main.cpp:84-113).  Each mesh's result is exactly slak_subdivide's on
  * that mesh alone.  All sizes are fixed at creation (one stream sync for all
  * meshes' level-0 topology); every output lives in one batch-owned buffer
- * (slak_batch_output returns views, valid until slak_batch_destroy); plans
- * share device scratch in waves sized to the free memory; within a wave,
- * meshes run concurrently on parallel streams.  With SLAK_PLAN_GRAPH the whole
- * batch is captured as one CUDA graph on the first execution.
+ * (slak_batch_output returns views, valid until slak_batch_destroy).
+ *
+ * Meshes that refine to fewer than 2^19 quads (SLAK_BATCH_GROUP_QUADS in the
+ * environment at creation overrides the bound; 0 turns groups off) run in
+ * groups: meshes whose plans launch the same kernels with the same shapes in
+ * the same order, each step one grouped launch over all of them (a block finds
+ * its mesh in a table of block offsets).  A small mesh's ~18 launches become a
+ * share of its group's, so a batch of many small meshes is no longer bound by
+ * launches.  Each grouped mesh has its own scratch; together they take at
+ * most half of the scratch budget.  The other meshes run in 16 concurrent
+ * chains, dealt longest predicted time first to the least loaded chain; a
+ * chain reuses one scratch slice for its meshes.  Only when the chains'
+ * slices outgrow the budget (3/4 of the free memory after the outputs, at most
+ * 24 GB; SLAK_BATCH_WAVE_BYTES overrides the cap) does the batch run in
+ * several waves.  With SLAK_PLAN_GRAPH the whole batch is captured as one
+ * CUDA graph on the first execution.
  */
 typedef struct slak_batch slak_batch;
 int slak_batch_create(const slak_mesh* meshes, const int* levels, int64_t count, int scheme, int flags,
@@ -351,8 +363,9 @@ int slak_batch_execute(slak_batch* batch, slak_stream_t stream);
 int slak_batch_status(slak_batch* batch, slak_stream_t stream);
 /* The refined mesh of meshes[index]; left untouched when that mesh had nothing to refine. */
 int slak_batch_output(const slak_batch* batch, int64_t index, slak_mesh* rmesh);
-int slak_batch_num_waves(const slak_batch* batch);
-int64_t slak_batch_launches(const slak_batch* batch);
+int slak_batch_num_waves(const slak_batch* batch);     /* waves of the chained meshes        */
+int slak_batch_num_groups(const slak_batch* batch);    /* groups of small meshes              */
+int64_t slak_batch_launches(const slak_batch* batch);  /* kernel launches of one execution    */
 int slak_batch_destroy(slak_batch* batch);
 
 /*
@@ -362,7 +375,7 @@ int slak_batch_destroy(slak_batch* batch);
  * cudaMalloc and belongs to the caller, who frees it with slak_mesh_free or
  * cudaFree, as after slak_subdivide. A mesh with nothing to refine leaves
  * rmeshes[i] zeroed. The call returns once every mesh is refined. All
- * outputs are resident at once; the scratch runs in waves.
+ * outputs are resident at once; the scratch is shared as in slak_batch_create.
  */
 int slak_subdivide_batched(const slak_mesh* meshes, const int* levels, int64_t count, int scheme,
                            slak_mesh* rmeshes, slak_stream_t stream);

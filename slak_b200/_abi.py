@@ -33,7 +33,7 @@ EXPORTS = ["slak_status_string", "slak_abi_version", "slak_last_error_detail", "
            "slak_plan_num_levels", "slak_plan_level_stats", "slak_plan_launches", "slak_plan_kernel_timings",
            "slak_plan_tuning", "slak_autotune_reset",
            "slak_plan_destroy", "slak_subdivide_batched", "slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
-           "slak_batch_num_waves", "slak_batch_launches", "slak_batch_destroy"]
+           "slak_batch_num_waves", "slak_batch_num_groups", "slak_batch_launches", "slak_batch_destroy"]
 
 
 class SlakCorners(ctypes.Structure):
@@ -142,11 +142,12 @@ def lib():
         L.slak_batch_status.argtypes = [V, V]
         L.slak_batch_output.argtypes = [V, I64, P]
         L.slak_batch_num_waves.argtypes = [V]
+        L.slak_batch_num_groups.argtypes = [V]
         L.slak_batch_launches.argtypes = [V]
         L.slak_batch_launches.restype = I64
         L.slak_batch_destroy.argtypes = [V]
         for n in ("slak_batch_create", "slak_batch_execute", "slak_batch_status", "slak_batch_output",
-                  "slak_batch_num_waves", "slak_batch_destroy"):
+                  "slak_batch_num_waves", "slak_batch_num_groups", "slak_batch_destroy"):
             getattr(L, n).restype = I
         for n in ("slak_subdivide", "slak_mesh_free", "slak_subdivide_level_noalloc", "slak_plan_create",
                   "slak_plan_create_creased", "slak_subdivide_creased", "slak_plan_create_sharp",

@@ -355,6 +355,10 @@ class Batch:
         return int(_abi.lib().slak_batch_num_waves(self._h))
 
     @property
+    def groups(self) -> int:
+        return int(_abi.lib().slak_batch_num_groups(self._h))
+
+    @property
     def launches(self) -> int:
         return int(_abi.lib().slak_batch_launches(self._h))
 

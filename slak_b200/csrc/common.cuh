@@ -7,7 +7,10 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
+#include <type_traits>
 #include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace slak {
@@ -49,6 +52,142 @@ inline void launch_k(void (*kernel)(KArgs...), unsigned grid, unsigned block, cu
     cfg.attrs = at;
     cfg.numAttrs = kUsePdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// ---------------------------------------------------------- grouped launches
+// Every kernel a plan launches is written as a body, a __device__ function of
+// its block index (k_*_body); a __global__ wrapper (k_*) runs it for
+// blockIdx.x, and a group functor (k_*_g) names it for grouped launches.  A
+// grouped launch runs one kernel for many meshes at once: its grid is the
+// meshes' grids end to end, and each block finds its mesh in a table of block
+// offsets (binary search) and its arguments in an array of argument packs.
+// A batch records the launches of its small meshes' plans (launch_g with
+// g_record set) and replays each step of a group of plans with identical
+// launch sequences as one grouped launch.
+
+// The arguments of one launch, trivially copyable, in one block of bytes.
+template <size_t I, class T> struct PackLeaf { T v; };
+template <class Seq, class... A> struct PackImpl;
+template <size_t... I, class... A>
+struct PackImpl<std::index_sequence<I...>, A...> : PackLeaf<I, A>... {
+    PackImpl() = default;
+    explicit PackImpl(const A&... a) : PackLeaf<I, A>{a}... {}
+};
+template <class... A> using Pack = PackImpl<std::index_sequence_for<A...>, A...>;
+
+template <class G, size_t... I, class... A>
+__device__ __forceinline__ void run_pack(unsigned bx, const PackImpl<std::index_sequence<I...>, A...>& p)
+{
+    G{}(bx, static_cast<const PackLeaf<I, A>&>(p).v...);
+}
+
+// the mesh whose block range [bstart[m], bstart[m+1]) holds this block
+__device__ __forceinline__ int group_mesh(const unsigned* __restrict__ bstart, int nm)
+{
+    int lo = 0, hi = nm - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(bstart + mid) <= blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// G::kBounds: the launch bounds of the kernel's own wrapper (0 none, 1 the
+// block size, 2 the block size and blocks per SM), repeated here
+template <class G, class P>
+__global__ void k_group(const P* __restrict__ args, const unsigned* __restrict__ bstart, int nm)
+{
+    griddep_enter();
+    const int m = group_mesh(bstart, nm);
+    run_pack<G>(blockIdx.x - __ldg(bstart + m), args[m]);
+}
+template <class G, class P>
+__global__ void __launch_bounds__(G::kMaxT) k_group_t(const P* __restrict__ args, const unsigned* __restrict__ bstart,
+                                                      int nm)
+{
+    griddep_enter();
+    const int m = group_mesh(bstart, nm);
+    run_pack<G>(blockIdx.x - __ldg(bstart + m), args[m]);
+}
+template <class G, class P>
+__global__ void __launch_bounds__(G::kMaxT, G::kMinB) k_group_b(const P* __restrict__ args,
+                                                                const unsigned* __restrict__ bstart, int nm)
+{
+    griddep_enter();
+    const int m = group_mesh(bstart, nm);
+    run_pack<G>(blockIdx.x - __ldg(bstart + m), args[m]);
+}
+
+using GroupLaunchFn = void (*)(const void* args, const unsigned* bstart, int nm, unsigned grid, unsigned block,
+                               cudaStream_t s);
+
+template <class G, class P>
+void group_launch(const void* args, const unsigned* bstart, int nm, unsigned grid, unsigned block, cudaStream_t s)
+{
+    const P* a = static_cast<const P*>(args);
+    if constexpr (G::kBounds == 2) launch_k(k_group_b<G, P>, grid, block, s, a, bstart, nm);
+    else if constexpr (G::kBounds == 1) launch_k(k_group_t<G, P>, grid, block, s, a, bstart, nm);
+    else launch_k(k_group<G, P>, grid, block, s, a, bstart, nm);
+}
+
+// One recorded launch: the grouped launcher of its kernel and argument types
+// (which identifies it), its shape and its argument pack.
+struct RecLaunch {
+    GroupLaunchFn fn = nullptr;
+    unsigned grid = 0, block = 0;
+    size_t align = 0;
+    std::vector<unsigned char> pack;
+};
+inline thread_local std::vector<RecLaunch>* g_record = nullptr;
+
+template <class G, class... Args>
+inline void launch_g(unsigned grid, unsigned block, cudaStream_t s, Args&&... args)
+{
+    if (g_record) {
+        using P = Pack<std::decay_t<Args>...>;
+        static_assert(std::is_trivially_copyable<P>::value, "launch arguments must be trivially copyable");
+        const P pk(args...);
+        RecLaunch r;
+        r.fn = &group_launch<G, P>;
+        r.grid = grid;
+        r.block = block;
+        r.align = alignof(P);
+        r.pack.resize(sizeof(P));
+        std::memcpy(r.pack.data(), &pk, sizeof(P));
+        g_record->push_back(std::move(r));
+        return;
+    }
+    launch_k(G::kernel(), grid, block, s, std::forward<Args>(args)...);
+}
+
+// n int32 words set to 0 (the plans' status words and counters)
+__device__ __forceinline__ void k_zero_body(const unsigned bx_, int* __restrict__ p, int64_t n)
+{
+    const int64_t i = (int64_t)bx_ * kBlock + threadIdx.x;
+    if (i < n) p[i] = 0;
+}
+__global__ void __launch_bounds__(kBlock) k_zero(int* __restrict__ p, int64_t n)
+{
+    griddep_enter();
+    k_zero_body(blockIdx.x, p, n);
+}
+struct k_zero_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const { k_zero_body(bx, a...); }
+    static constexpr auto kernel() { return &k_zero; }
+};
+
+// cudaMemsetAsync to 0 of `bytes` (a multiple of 4), or its grouped form
+inline void zero_async(void* p, size_t bytes, cudaStream_t s)
+{
+    if (g_record) {
+        const int64_t n = (int64_t)(bytes / 4);
+        launch_g<k_zero_g>((unsigned)((n + kBlock - 1) / kBlock > 0 ? (n + kBlock - 1) / kBlock : 1), kBlock, s,
+                           static_cast<int*>(p), n);
+        return;
+    }
+    cudaMemsetAsync(p, 0, bytes, s);
 }
 
 // ---------------------------------------------------------------- float4 ops

@@ -465,13 +465,12 @@ __device__ __forceinline__ int sg_sptr(const FastDims& d, const int* __restrict_
 // vals[q] = {1, 2, 3, 4}; they depend on q alone, so a block writes the 4 BS
 // refined quads of its span with consecutive threads (coalesced).
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
-__global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                           const float* __restrict__ P, QState p, QState c,
-                                           int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
-                                           int* __restrict__ optr, int4* __restrict__ ovals)
+__device__ __forceinline__ void k_g1_body(const unsigned bx_, FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                                              const float* __restrict__ P, QState p, QState c,
+                                                              int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
+                                                              int* __restrict__ optr, int4* __restrict__ ovals)
 {
-    griddep_enter();
-    const int x0 = blockIdx.x * blockDim.x;
+    const int x0 = bx_ * blockDim.x;
     const int x = x0 + threadIdx.x;
     const bool valid = x < d.N1;
     const int lane = threadIdx.x & 31, q = x & 3;
@@ -744,6 +743,24 @@ __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, F
         if (x == 0) optr[d.N] = 4 * d.N;
     }
 }
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
+__global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                                                   const float* __restrict__ P, QState p, QState c,
+                                                                   int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
+                                                                   int* __restrict__ optr, int4* __restrict__ ovals)
+{
+    griddep_enter();
+    k_g1_body<LAK, STATE, PQ, BS, BND, GQ, SG>(blockIdx.x, d, pf, ids, P, p, c, out_ids, R, z, optr, ovals);
+}
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
+struct k_g1_g {
+    static constexpr int kBounds = 2, kMaxT = BS, kMinB = (GQ ? 768 : 1024) / BS;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_g1_body<LAK, STATE, PQ, BS, BND, GQ, SG>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_g1<LAK, STATE, PQ, BS, BND, GQ, SG>; }
+};
 
 // ---------------------------------------------------------------------------------------------
 // The vertex point of P's face point with the face's k > 4 corners b..e-1 under
@@ -782,12 +799,11 @@ __device__ __noinline__ float4 face_vertex_compensated(const int* __restrict__ i
 // edges {face point, e_in(x)}: the work k_g1 does with shuffles when P's faces
 // are quads.  Same formulas and order, with n = k.
 template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
-                                               const float* __restrict__ P, QState c, float* __restrict__ R,
-                                               int compensated)
+__device__ __forceinline__ void k_gf_body(const unsigned bx_, FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
+                                                              const float* __restrict__ P, QState c, float* __restrict__ R,
+                                                              int compensated)
 {
-    griddep_enter();
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = bx_ * blockDim.x + threadIdx.x;
     if (g >= d.F1) return;
     const int b = __ldg(pptr + g), e = __ldg(pptr + g + 1), k = e - b;
     const float4 c2 = ldg4(P, d.V1 + g);
@@ -879,6 +895,23 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
     st4(R, (int64_t)d.V1 + g, yv);
     if (STATE) c.sptr[d.V1 + g] = d.N1 + b;
 }
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
+                                               const float* __restrict__ P, QState c, float* __restrict__ R,
+                                               int compensated)
+{
+    griddep_enter();
+    k_gf_body<LAK, STATE>(blockIdx.x, d, pptr, ids, P, c, R, compensated);
+}
+template <bool LAK, bool STATE>
+struct k_gf_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_gf_body<LAK, STATE>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_gf<LAK, STATE>; }
+};
 
 // ---------------------------------------------------------------------------------------------
 // G2 (polygon P; with quad P k_g1 does this work): the edges of P, visited in
@@ -890,11 +923,10 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
 // face's three (its face point, C's face points of quads h2 and next(h2)) are
 // gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
-__global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                           const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
+__device__ __forceinline__ void k_g2_body(const unsigned bx_, FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                                              const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
 {
-    griddep_enter();
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int x = bx_ * blockDim.x + threadIdx.x;
     const bool valid = x < d.N1;
     const int lane = threadIdx.x & 31, q = x & 3;
     const int ln = (lane & ~3) | ((q + 1) & 3);
@@ -932,6 +964,22 @@ __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* 
     edge_point_vertex<LAK, STATE, BND>(d, c, R, h, nh, h2, nh2, ve, fh, fh2, Pv, Pu, Pe, Pf, Pf2, Fh, Fnh, Fh2, Fnh2,
                                        br);
 }
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
+__global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
+                                           const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
+{
+    griddep_enter();
+    k_g2_body<LAK, STATE, PQ, BS, BND>(blockIdx.x, d, pf, ids, P, p, c, R);
+}
+template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
+struct k_g2_g {
+    static constexpr int kBounds = 1, kMaxT = BS, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_g2_body<LAK, STATE, PQ, BS, BND>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_g2<LAK, STATE, PQ, BS, BND>; }
+};
 
 // ---------------------------------------------------------------------------------------------
 // A vertex of P on C's boundary (a slot of its column has a half-edge without
@@ -1208,11 +1256,10 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
 // `nv`: the vertices of P it covers, V1 (or V2 on a GQ level, whose other
 // columns k_g1 sums).
 template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
-__global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
-                                           SlotScratch z, float* __restrict__ R, int compensated, int nv)
+__device__ __forceinline__ void k_g3_body(const unsigned bx_, FastDims d, const float* __restrict__ P, QState p, QState c,
+                                                              SlotScratch z, float* __restrict__ R, int compensated, int nv)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     if (STATE && v == nv) c.sptr[d.V] = d.N;
     const bool valid = v < nv;
     int b = 0, n = 0;
@@ -1230,6 +1277,22 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
                                         __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
     }
 }
+template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
+__global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__ P, QState p, QState c,
+                                           SlotScratch z, float* __restrict__ R, int compensated, int nv)
+{
+    griddep_enter();
+    k_g3_body<LAK, STATE, BS, BND, SG>(blockIdx.x, d, P, p, c, z, R, compensated, nv);
+}
+template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
+struct k_g3_g {
+    static constexpr int kBounds = 1, kMaxT = BS, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_g3_body<LAK, STATE, BS, BND, SG>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_g3<LAK, STATE, BS, BND, SG>; }
+};
 
 // ---------------------------------------------------------------------------------------------
 // k_g3 with its block's slot records staged in shared memory by the bulk-copy
@@ -1260,15 +1323,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int pol
 }
 
 template <bool LAK, bool STATE>
-__global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float* __restrict__ P, QState p,
-                                                        QState c, SlotScratch z, float* __restrict__ R,
-                                                        int compensated, int nv, DevStatus* st, int polls)
+__device__ __forceinline__ void k_g3_bulk_body(const unsigned bx_, FastDims d, const float* __restrict__ P, QState p,
+                                                                   QState c, SlotScratch z, float* __restrict__ R,
+                                                                   int compensated, int nv, DevStatus* st, int polls)
 {
-    griddep_enter();
     __shared__ __align__(128) float4 zs[2 * kBulkSlots];
     __shared__ __align__(16) int rs[kBulkSlots + 8];
     __shared__ __align__(8) unsigned long long bar;
-    const int v0 = blockIdx.x * kBulkBlock, v = v0 + threadIdx.x;
+    const int v0 = bx_ * kBulkBlock, v = v0 + threadIdx.x;
     if (STATE && v == nv) c.sptr[d.V] = d.N;
     if (v0 >= nv) return;                                   // the sentinel's block
     const int vl = min(v0 + kBulkBlock, nv);
@@ -1297,7 +1359,7 @@ __global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float*
         }
         // the warp decides together (the column pass below shuffles across it)
         if (!__all_sync(0xffffffffu, mbar_wait(sbar, 0, polls))) {
-            if ((threadIdx.x & 31) == 0) set_error(st, 5, 3000000 + blockIdx.x);     // SLAK_ERR_TIMEOUT
+            if ((threadIdx.x & 31) == 0) set_error(st, 5, 3000000 + bx_);     // SLAK_ERR_TIMEOUT
             mbar_wait(sbar, 0, kBulkRetire);
             return;
         }
@@ -1328,17 +1390,46 @@ __global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float*
                                           __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
     }
 }
+template <bool LAK, bool STATE>
+__global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float* __restrict__ P, QState p,
+                                                        QState c, SlotScratch z, float* __restrict__ R,
+                                                        int compensated, int nv, DevStatus* st, int polls)
+{
+    griddep_enter();
+    k_g3_bulk_body<LAK, STATE>(blockIdx.x, d, P, p, c, z, R, compensated, nv, st, polls);
+}
+template <bool LAK, bool STATE>
+struct k_g3_bulk_g {
+    static constexpr int kBounds = 1, kMaxT = kBulkBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_g3_bulk_body<LAK, STATE>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_g3_bulk<LAK, STATE>; }
+};
 
 // ---------------------------------------------------------------------------------------------
 // 1 for each edge of a general level without a twin (H holds -1), the input of
 // the scan that gives the edges' boundary ranks to the first fast level
-__global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restrict__ isb)
+__device__ __forceinline__ void k_export_bflag_body(const unsigned bx_, int E, const int2* __restrict__ H, int* __restrict__ isb)
 {
-    griddep_enter();
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    int e = bx_ * blockDim.x + threadIdx.x;
     if (e >= E) return;
     const int2 h = H[e];
     isb[e] = (h.x < 0) | (h.y < 0);
 }
+__global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restrict__ isb)
+{
+    griddep_enter();
+    k_export_bflag_body(blockIdx.x, E, H, isb);
+}
+struct k_export_bflag_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_export_bflag_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_export_bflag; }
+};
 
 }  // namespace slak

@@ -31,11 +31,10 @@ enum : int { SF_OWNER = 1, SF_BOUT = 2, SF_BIN = 4 };
 
 // polygon levels: corner -> face (validating ptr) and the valences in one pass
 // over the faces
-__global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
-                                   int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
+__device__ __forceinline__ void k_face_map_valence_body(const unsigned bx_, const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
+                                                                            int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
 {
-    griddep_enter();
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = bx_ * blockDim.x + threadIdx.x;
     if (f == 0 && (ptr[0] != 0 || ptr[F] != N)) set_error(st, 4, -1);
     if (f >= F) return;
     int b = ptr[f], e = ptr[f + 1];
@@ -47,47 +46,98 @@ __global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __res
         atomicAdd(cnt + v, 1);
     }
 }
-
-__global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
+__global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
+                                   int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
 {
     griddep_enter();
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    k_face_map_valence_body(blockIdx.x, ptr, ids, F, N, V, cface, cnt, st);
+}
+struct k_face_map_valence_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_face_map_valence_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_face_map_valence; }
+};
+
+__device__ __forceinline__ void k_valence_body(const unsigned bx_, const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
+{
+    int c = bx_ * blockDim.x + threadIdx.x;
     if (c >= N) return;
     int v = ids[c];
     if ((unsigned)v >= (unsigned)V) { set_error(st, 4, c); return; }
     atomicAdd(cnt + v, 1);
 }
+__global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __restrict__ cnt, DevStatus* st)
+{
+    griddep_enter();
+    k_valence_body(blockIdx.x, ids, N, V, cnt, st);
+}
+struct k_valence_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_valence_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_valence; }
+};
 
 // valence histogram (0..15, 16 or more): the autotuner's key, read with the
 // level-0 probe
-__global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restrict__ hist)
+__device__ __forceinline__ void k_valence_hist_body(const unsigned bx_, int V, const int* __restrict__ sptr, int* __restrict__ hist)
 {
-    griddep_enter();
     __shared__ int h[17];
     if (threadIdx.x < 17) h[threadIdx.x] = 0;
     __syncthreads();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     if (v < V) atomicAdd(&h[min(sptr[v + 1] - sptr[v], 16)], 1);
     __syncthreads();
     if (threadIdx.x < 17 && h[threadIdx.x]) atomicAdd(hist + threadIdx.x, h[threadIdx.x]);
 }
+__global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restrict__ hist)
+{
+    griddep_enter();
+    k_valence_hist_body(blockIdx.x, V, sptr, hist);
+}
+struct k_valence_hist_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_valence_hist_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_valence_hist; }
+};
 
 // slot order from the atomic is arbitrary (the unsorted column goes to
 // `loose`); k_vsort makes it canonical.  A malformed polygon mesh (a face the
 // valence pass rejected, or corners past ptr[F]) brings more corners to a
 // vertex than its column counts: those find no slot (r < 0) and are dropped,
 // so nothing is written outside the column; the level fails with BAD_MESH.
-__global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
-                         int* __restrict__ fill, int* __restrict__ loose)
+__device__ __forceinline__ void k_bucket_body(const unsigned bx_, const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
+                                                                  int* __restrict__ fill, int* __restrict__ loose)
 {
-    griddep_enter();
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = bx_ * blockDim.x + threadIdx.x;
     if (c >= N) return;
     int v = ids[c];
     if ((unsigned)v >= (unsigned)V) return;
     int r = atomicSub(fill + v, 1) - 1;
     if (r >= 0) loose[sptr[v] + r] = c;
 }
+__global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
+                         int* __restrict__ fill, int* __restrict__ loose)
+{
+    griddep_enter();
+    k_bucket_body(blockIdx.x, ids, N, V, sptr, fill, loose);
+}
+struct k_bucket_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_bucket_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_bucket; }
+};
 
 // Each column sorted by corner index: a corner's slot is the number of smaller
 // corners in its column (corner indices are distinct).  Columns of up to 8 are
@@ -106,12 +156,11 @@ __device__ __forceinline__ void vsort_neighbours(Faces<QUAD> fc, const int* __re
 }
 
 template <bool QUAD>
-__global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
-                        const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
-                        int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
+__device__ __forceinline__ void k_vsort_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
+                                                                 const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
+                                                                 int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int b = 0, n = 0;
     if (v < V) { b = sptr[v]; n = sptr[v + 1] - b; }
@@ -146,6 +195,23 @@ __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, cons
         }
     }
 }
+template <bool QUAD>
+__global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
+                        const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
+                        int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
+{
+    griddep_enter();
+    k_vsort_body<QUAD>(blockIdx.x, fc, ids, V, sptr, loose, sc, snext, sprev, sprevc, xslot);
+}
+template <bool QUAD>
+struct k_vsort_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_vsort_body<QUAD>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_vsort<QUAD>; }
+};
 
 // Twins and boundary flags from the vertex's own column: the outgoing
 // half-edge v->w of slot s has a twin iff some corner at v is entered from w.
@@ -206,13 +272,12 @@ struct ColRegs {         // a column of at most 8 slots in registers
 // slot per lane, so no thread walks n^2 pairs alone.
 // With `xtw` the twin of every corner is exported as well (corner -> twin).
 template <bool LAK>
-__global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                        const int* __restrict__ snext, const int* __restrict__ sprev,
-                        const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
-                        int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
+__device__ __forceinline__ void k_edges_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                                                                 const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                                 const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
+                                                                 int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     int nb = 0, b = 0, n = 0;
     if (v < V) { b = sptr[v]; n = sptr[v + 1] - b; }
@@ -268,6 +333,24 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
     for (int o = 16; o > 0; o >>= 1) nb += __shfl_down_sync(0xffffffffu, nb, o);
     if (lane == 0 && nb) atomicAdd(bcount, nb);
 }
+template <bool LAK>
+__global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                        const int* __restrict__ snext, const int* __restrict__ sprev,
+                        const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
+                        int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
+{
+    griddep_enter();
+    k_edges_body<LAK>(blockIdx.x, V, sptr, sc, snext, sprev, sprevc, stw, sflag, ecnt, bcount, xtw, st);
+}
+template <bool LAK>
+struct k_edges_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_edges_body<LAK>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_edges<LAK>; }
+};
 
 // SLAK edge ids: owners in slot order get eptr[v] + rank; the twin shares it.
 // Thread 0 of k_eids_* also checks the level's edge and boundary counts
@@ -278,13 +361,12 @@ __device__ __forceinline__ void check_level(int v, const int* eptr, int V, int E
     if (v == 0 && (eptr[V] != E || *bcount != B)) set_error(st, 4, 1000 + li);
 }
 
-__global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                            const int* __restrict__ stw, const int* __restrict__ sflag,
-                            const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
-                            int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
+__device__ __forceinline__ void k_eids_slak_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                                                                     const int* __restrict__ stw, const int* __restrict__ sflag,
+                                                                     const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                                                                     int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
 {
-    griddep_enter();
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    int v = bx_ * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
     if (v >= V) return;
     int id = eptr[v];
@@ -298,6 +380,22 @@ __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __re
         ++id;
     }
 }
+__global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                            const int* __restrict__ stw, const int* __restrict__ sflag,
+                            const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                            int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
+{
+    griddep_enter();
+    k_eids_slak_body(blockIdx.x, V, sptr, sc, stw, sflag, eptr, Ecap, eid, H, st, bcount, B, li);
+}
+struct k_eids_slak_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_eids_slak_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_eids_slak; }
+};
 
 // LAK edge ids of one vertex's column on its own thread
 __device__ __forceinline__ void eids_lak_vertex(const int* __restrict__ sc, const int* __restrict__ snext,
@@ -402,14 +500,13 @@ __device__ __noinline__ void eids_lak_warp(const int* __restrict__ sc, const int
 // LAK edge ids: ascending (max, min); H = (half-edge min->max, half-edge
 // max->min), -1 where one is missing.  Columns longer than kBigCol go to
 // their warp.
-__global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                           const int* __restrict__ snext, const int* __restrict__ sprev,
-                           const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
-                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
-                           int li)
+__device__ __forceinline__ void k_eids_lak_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                                                                    const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                                    const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
+                                                                    int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
+                                                                    int li)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
     const bool valid = v < V;
     int b = 0, n = 0;
@@ -424,18 +521,34 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
                       __shfl_sync(0xffffffffu, b, src), __shfl_sync(0xffffffffu, n, src));
     }
 }
+__global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                           const int* __restrict__ snext, const int* __restrict__ sprev,
+                           const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
+                           int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
+                           int li)
+{
+    griddep_enter();
+    k_eids_lak_body(blockIdx.x, V, sptr, sc, snext, sprev, sprevc, eptr, Ecap, eid, H, st, bcount, B, li);
+}
+struct k_eids_lak_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_eids_lak_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_eids_lak; }
+};
 
 // refined quad of corner c: {v, V+F+e_out, V+face, V+F+e_in}
 // With `xt` (a SLAK level whose state feeds the fast path) it also exports
 // t[c] = slot[twin(prev c)], -1 where prev(c) has no twin.
 template <bool QUAD, bool LAK>
-__global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
-                         int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
-                         int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
-                         int* __restrict__ xt)
+__device__ __forceinline__ void k_refine_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
+                                                                  int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
+                                                                  int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
+                                                                  int* __restrict__ xt)
 {
-    griddep_enter();
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = bx_ * blockDim.x + threadIdx.x;
     if (c >= N) return;
     const int VF = V + F;
     const int p = fc.prev(c);
@@ -451,32 +564,62 @@ __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int*
         if (c == N - 1) out_ptr[N] = 4 * N;
     }
 }
+template <bool QUAD, bool LAK>
+__global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
+                         int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
+                         int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
+                         int* __restrict__ xt)
+{
+    griddep_enter();
+    k_refine_body<QUAD, LAK>(blockIdx.x, fc, ids, eid, N, V, F, out_ids, out_ptr, out_vals, xslot, xtw, xt);
+}
+template <bool QUAD, bool LAK>
+struct k_refine_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_refine_body<QUAD, LAK>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_refine<QUAD, LAK>; }
+};
 
 // ------------------------------------------------------------------ positions
 
 // SLAK quad face point: ((c0 + c2) + (c1 + c3)) * 1/4, the pairing of the
 // width-16 shuffles in calculateFaceEdgepointsQuad (CatmullClarkKernels.cuh:586-594)
-__global__ void k_fp_slak_quad(const int4* __restrict__ ids4, const float* __restrict__ P, int F,
-                               float* __restrict__ FP)
+__device__ __forceinline__ void k_fp_slak_quad_body(const unsigned bx_, const int4* __restrict__ ids4, const float* __restrict__ P, int F,
+                                                                        float* __restrict__ FP)
 {
-    griddep_enter();
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = bx_ * blockDim.x + threadIdx.x;
     if (f >= F) return;
     int4 q = __ldg(ids4 + f);
     float4 a = ldg4(P, q.x), b = ldg4(P, q.y), c = ldg4(P, q.z), d = ldg4(P, q.w);
     st4(FP, f, f4_mul(f4_add(f4_add(a, c), f4_add(b, d)), 0.25f));
 }
+__global__ void k_fp_slak_quad(const int4* __restrict__ ids4, const float* __restrict__ P, int F,
+                               float* __restrict__ FP)
+{
+    griddep_enter();
+    k_fp_slak_quad_body(blockIdx.x, ids4, P, F, FP);
+}
+struct k_fp_slak_quad_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_fp_slak_quad_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_fp_slak_quad; }
+};
 
 // polygon face point: sum from zero in corner order, then
 //   SLAK: times the rounded reciprocal of the order (calculateFacepoints, :602-618)
 //   LAK:  divided by the order, plus 0 (spmv_left_mapped_f4 + divElementWise,
 //         LAKCatmullClarkImpl.cu:175-178)
 template <bool QUAD, bool LAK>
-__global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
-                         int F, float* __restrict__ FP)
+__device__ __forceinline__ void k_fp_seq_body(const unsigned bx_, const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
+                                                                  int F, float* __restrict__ FP)
 {
-    griddep_enter();
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = bx_ * blockDim.x + threadIdx.x;
     if (f >= F) return;
     int b = QUAD ? 4 * f : ptr[f], e = QUAD ? 4 * f + 4 : ptr[f + 1];
     float4 acc = f4_zero();
@@ -484,6 +627,22 @@ __global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ id
     float n = (float)(e - b);
     st4(FP, f, LAK ? f4_div_z(acc, n) : f4_mul(acc, __fdiv_rn(1.0f, n)));
 }
+template <bool QUAD, bool LAK>
+__global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
+                         int F, float* __restrict__ FP)
+{
+    griddep_enter();
+    k_fp_seq_body<QUAD, LAK>(blockIdx.x, ptr, ids, P, F, FP);
+}
+template <bool QUAD, bool LAK>
+struct k_fp_seq_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_fp_seq_body<QUAD, LAK>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_fp_seq<QUAD, LAK>; }
+};
 
 // edge points.  SLAK: 0 + (p_a + fp_a)/4 + (p_b + fp_b)/4 over the two
 // half-edges (calculateFaceEdgepointsQuad :597-599, calculateEdgepoints
@@ -491,11 +650,10 @@ __global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ id
 // LAK: (((p_min + p_max) + fp(min->max)) + fp(max->min)) / 4, boundary midpoint
 // (calculateInternal/ExternalEdgepoints, LAKCatmullClarkKernels.cuh:437-462).
 template <bool QUAD, bool LAK>
-__global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
-                     const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
+__device__ __forceinline__ void k_ep_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
+                                                              const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
 {
-    griddep_enter();
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    int e = bx_ * blockDim.x + threadIdx.x;
     if (e >= E) return;
     int2 h = __ldg(H + e);
     float4 r;
@@ -518,6 +676,22 @@ __global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __
     }
     st4_cs(EP, e, r);
 }
+template <bool QUAD, bool LAK>
+__global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
+                     const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
+{
+    griddep_enter();
+    k_ep_body<QUAD, LAK>(blockIdx.x, fc, ids, H, E, P, FP, EP);
+}
+template <bool QUAD, bool LAK>
+struct k_ep_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_ep_body<QUAD, LAK>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_ep<QUAD, LAK>; }
+};
 
 // SLAK boundary vertex: 3/4 p + 1/8 next (first out-boundary slot) + 1/8 prev
 // (first in-boundary slot); y unchanged when v has no boundary slot
@@ -606,13 +780,12 @@ __device__ __noinline__ void vp_slak_warp(Faces<QUAD> fc, const int* __restrict_
 // becomes 3/4 p + 1/8 next + 1/8 prev (correctBoundaryS1/S2, :688-740).
 // Columns longer than kBigCol go to their warp.
 template <bool QUAD>
-__global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                          const int* __restrict__ snext, const int* __restrict__ sprev,
-                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
-                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
+__device__ __forceinline__ void k_vp_slak_body(const unsigned bx_, Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                                                                   const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                                   const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                                                                   const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     const bool valid = v < V;
     int b = 0, n = 0;
     if (valid) { b = sptr[v]; n = sptr[v + 1] - b; }
@@ -627,6 +800,24 @@ __global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, c
                            __shfl_sync(0xffffffffu, n, src));
     }
 }
+template <bool QUAD>
+__global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                          const int* __restrict__ snext, const int* __restrict__ sprev,
+                          const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                          const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    griddep_enter();
+    k_vp_slak_body<QUAD>(blockIdx.x, fc, V, sptr, sc, snext, sprev, sflag, boundary, P, FP, R, compensated);
+}
+template <bool QUAD>
+struct k_vp_slak_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_vp_slak_body<QUAD>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_vp_slak<QUAD>; }
+};
 
 // LAK boundary vertex: 3/4 p + 1/8 p_other per boundary edge in edge-id order;
 // y unchanged when v has no boundary slot
@@ -762,14 +953,13 @@ __device__ __noinline__ void vp_lak_warp(Faces<QUAD> fc, const int* __restrict__
 // (prepare/calculateExternalVertexUpdate, LAKCatmullClarkKernels.cuh:464-511).
 // Columns longer than kBigCol go to their warp.
 template <bool QUAD>
-__global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                         const int* __restrict__ snext, const int* __restrict__ sprev,
-                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
-                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
-                         const float* __restrict__ FP, float* __restrict__ R, int compensated)
+__device__ __forceinline__ void k_vp_lak_body(const unsigned bx_, Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                                                                  const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                                  const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                                                                  const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                                                                  const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
-    griddep_enter();
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx_ * blockDim.x + threadIdx.x;
     const bool valid = v < V;
     int b = 0, n = 0;
     if (valid) { b = sptr[v]; n = sptr[v + 1] - b; }
@@ -785,5 +975,24 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
                           __shfl_sync(0xffffffffu, n, src));
     }
 }
+template <bool QUAD>
+__global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
+                         const int* __restrict__ snext, const int* __restrict__ sprev,
+                         const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                         const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                         const float* __restrict__ FP, float* __restrict__ R, int compensated)
+{
+    griddep_enter();
+    k_vp_lak_body<QUAD>(blockIdx.x, fc, V, sptr, sc, snext, sprev, sprevc, sflag, eid, boundary, P, FP, R, compensated);
+}
+template <bool QUAD>
+struct k_vp_lak_g {
+    static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_vp_lak_body<QUAD>(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_vp_lak<QUAD>; }
+};
 
 }  // namespace slak

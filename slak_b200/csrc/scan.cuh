@@ -46,10 +46,9 @@ __device__ __forceinline__ int block_excl_scan(int x, int* total)
     return r;
 }
 
-__global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ tsum)
+__device__ __forceinline__ void k_scan_reduce_body(const unsigned bx_, const int* __restrict__ in, int64_t n, int* __restrict__ tsum)
 {
-    griddep_enter();
-    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    const int64_t base = (int64_t)bx_ * kScanTile;
     int s = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
@@ -59,13 +58,25 @@ __global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ 
     __shared__ int tot;
     block_excl_scan(s, &tot);
     __syncthreads();
-    if (threadIdx.x == 0) tsum[blockIdx.x] = tot;
+    if (threadIdx.x == 0) tsum[bx_] = tot;
 }
-
-// one block: exclusive scan of the tile sums in place, tsum[nt] = grand total
-__global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, int nt)
+__global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ tsum)
 {
     griddep_enter();
+    k_scan_reduce_body(blockIdx.x, in, n, tsum);
+}
+struct k_scan_reduce_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_scan_reduce_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_scan_reduce; }
+};
+
+// one block: exclusive scan of the tile sums in place, tsum[nt] = grand total
+__device__ __forceinline__ void k_scan_tiles_body(const unsigned bx_, int* __restrict__ tsum, int nt)
+{
     __shared__ int tot;
     int carry = 0;
     for (int base = 0; base < nt; base += kBlock) {
@@ -79,14 +90,26 @@ __global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, i
     }
     if (threadIdx.x == 0) tsum[nt] = carry;
 }
-
-__global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ in, int64_t n,
-                                                       const int* __restrict__ tsum, int nt, int* __restrict__ out)
+__global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, int nt)
 {
     griddep_enter();
+    k_scan_tiles_body(blockIdx.x, tsum, nt);
+}
+struct k_scan_tiles_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_scan_tiles_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_scan_tiles; }
+};
+
+__device__ __forceinline__ void k_scan_final_body(const unsigned bx_, const int* __restrict__ in, int64_t n,
+                                                                      const int* __restrict__ tsum, int nt, int* __restrict__ out)
+{
     __shared__ int tile[kScanTile];
     __shared__ int tot;
-    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    const int64_t base = (int64_t)bx_ * kScanTile;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         int j = i * kBlock + threadIdx.x;
@@ -98,7 +121,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ i
     int s = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) { loc[i] = s; s += tile[threadIdx.x * kScanItems + i]; }
-    int e = block_excl_scan(s, &tot) + tsum[blockIdx.x];
+    int e = block_excl_scan(s, &tot) + tsum[bx_];
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) tile[threadIdx.x * kScanItems + i] = e + loc[i];
     __syncthreads();
@@ -108,25 +131,38 @@ __global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ i
         int64_t k = base + j;
         if (k < n) out[k] = tile[j];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tsum[nt];
+    if (bx_ == 0 && threadIdx.x == 0) out[n] = tsum[nt];
 }
+__global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ in, int64_t n,
+                                                       const int* __restrict__ tsum, int nt, int* __restrict__ out)
+{
+    griddep_enter();
+    k_scan_final_body(blockIdx.x, in, n, tsum, nt, out);
+}
+struct k_scan_final_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_scan_final_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_scan_final; }
+};
 
 // Up to kScanSmallTiles tiles: no separate scan of the tile sums; each block
 // adds up the sums of the tiles before it (and all of them, for out[n]).
 constexpr int kScanSmallTiles = 2048;
 
-__global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restrict__ in, int64_t n,
-                                                             const int* __restrict__ tsum, int nt,
-                                                             int* __restrict__ out)
+__device__ __forceinline__ void k_scan_final_small_body(const unsigned bx_, const int* __restrict__ in, int64_t n,
+                                                                            const int* __restrict__ tsum, int nt,
+                                                                            int* __restrict__ out)
 {
-    griddep_enter();
     __shared__ int tile[kScanTile];
     __shared__ int tot;
     int before = 0, all = 0;
     for (int k = threadIdx.x; k < nt; k += kBlock) {
         const int x = tsum[k];
         all += x;
-        if (k < (int)blockIdx.x) before += x;
+        if (k < (int)bx_) before += x;
     }
     block_excl_scan(before, &tot);
     __syncthreads();
@@ -135,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restri
     block_excl_scan(all, &tot);
     __syncthreads();
     const int total = tot;
-    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    const int64_t base = (int64_t)bx_ * kScanTile;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         int j = i * kBlock + threadIdx.x;
@@ -157,8 +193,23 @@ __global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restri
         int64_t k = base + j;
         if (k < n) out[k] = tile[j];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = total;
+    if (bx_ == 0 && threadIdx.x == 0) out[n] = total;
 }
+__global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restrict__ in, int64_t n,
+                                                             const int* __restrict__ tsum, int nt,
+                                                             int* __restrict__ out)
+{
+    griddep_enter();
+    k_scan_final_small_body(blockIdx.x, in, n, tsum, nt, out);
+}
+struct k_scan_final_small_g {
+    static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    {
+        k_scan_final_small_body(bx, a...);
+    }
+    static constexpr auto kernel() { return &k_scan_final_small; }
+};
 
 inline int64_t scan_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
@@ -167,14 +218,14 @@ inline void scan_exclusive(const int* in, int* out, int64_t n, int* tmp, cudaStr
 {
     int64_t nt = scan_tiles(n);
     if (nt < 1) nt = 1;
-    launch_k(k_scan_reduce, (unsigned)nt, kBlock, s, in, n, tmp);
+    launch_g<k_scan_reduce_g>((unsigned)nt, kBlock, s, in, n, tmp);
     if (nt <= kScanSmallTiles) {
-        launch_k(k_scan_final_small, (unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
+        launch_g<k_scan_final_small_g>((unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
         if (launches) *launches += 2;
         return;
     }
-    launch_k(k_scan_tiles, 1, kBlock, s, tmp, (int)nt);
-    launch_k(k_scan_final, (unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
+    launch_g<k_scan_tiles_g>(1, kBlock, s, tmp, (int)nt);
+    launch_g<k_scan_final_g>((unsigned)nt, kBlock, s, in, n, tmp, (int)nt, out);
     if (launches) *launches += 3;
 }
 

@@ -270,20 +270,20 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
 {
     const int F = (int)L.F, V = (int)L.V, N = (int)L.N;
     cudaStream_t str = lc.s;
-    cudaMemsetAsync(s.cnt, 0, sizeof(int) * (size_t)V, str);
+    zero_async(s.cnt, sizeof(int) * (size_t)V, str);
     if (!L.quad) {
-        cudaMemsetAsync(s.cface, 0, sizeof(int) * (size_t)N, str);
-        launch_k(k_face_map_valence, grid_for(F), kBlock, str, L.ptr, L.ids, F, N, V, s.cface, s.cnt, st);
+        zero_async(s.cface, sizeof(int) * (size_t)N, str);
+        launch_g<k_face_map_valence_g>(grid_for(F), kBlock, str, L.ptr, L.ids, F, N, V, s.cface, s.cnt, st);
         lc.after("k_face_map_valence");
     } else {
-        launch_k(k_valence, grid_for(N), kBlock, str, L.ids, N, V, s.cnt, st);
+        launch_g<k_valence_g>(grid_for(N), kBlock, str, L.ids, N, V, s.cnt, st);
         lc.after("k_valence");
     }
     int64_t dummy = 0;
     scan_exclusive(s.cnt, s.sptr, V, s.tmp, str, &dummy);
     lc.after("scan(valence)", 3);
     // the unsorted columns live in sflag until k_edges writes the flags
-    launch_k(k_bucket, grid_for(N), kBlock, str, L.ids, N, V, s.sptr, s.cnt, s.sflag);
+    launch_g<k_bucket_g>(grid_for(N), kBlock, str, L.ids, N, V, s.sptr, s.cnt, s.sflag);
     lc.after("k_bucket");
     int* bcount = &st->bcount[li];
     // a general quad level feeding the fast path exports corner -> slot / twin
@@ -291,19 +291,19 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     int* xtw = L.export_state ? s.xtw : nullptr;
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
-        launch_k(k_vsort<true>, grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_g<k_vsort_g<true>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                                        s.sprevc, xslot);
     } else {
         Faces<false> fc{L.ptr, s.cface};
-        launch_k(k_vsort<false>, grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_g<k_vsort_g<false>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                                         s.sprevc, xslot);
     }
     lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
-        launch_k(k_edges<true>, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+        launch_g<k_edges_g<true>>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
                                                         s.sflag, s.ecnt, bcount, xtw, st);
     else
-        launch_k(k_edges<false>, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
+        launch_g<k_edges_g<false>>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
                                                          s.sflag, s.ecnt, bcount, xtw, st);
     lc.after("k_edges");
     scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, &dummy);
@@ -323,10 +323,10 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     Faces<QUAD> fc{L.ptr, s.cface};
     const int* bcount = &st->bcount[li];
     if (lak)
-        launch_k(k_eids_lak, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
+        launch_g<k_eids_lak_g>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
                                                      s.H, st, bcount, (int)L.B, li);
     else
-        launch_k(k_eids_slak, grid_for(V), kBlock, str, V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
+        launch_g<k_eids_slak_g>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
                                                       bcount, (int)L.B, li);
     lc.after("k_eids");
     // the refined quads (side stream 0) need only the edge ids; the positions
@@ -334,12 +334,12 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     if (lc.conc) lc.fork(0);
     cudaStream_t s_ref = lc.conc ? lc.side[0] : str;
     if (lak)
-        launch_k(k_refine<QUAD, true>, grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
+        launch_g<k_refine_g<QUAD, true>>(grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
                                                                 reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
                                                                 reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
                                                                 nullptr);
     else
-        launch_k(k_refine<QUAD, false>, grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
+        launch_g<k_refine_g<QUAD, false>>(grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
                                                                  reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
                                                                  s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
     lc.after("k_refine");
@@ -347,25 +347,25 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     float* FPo = R + 4 * (size_t)V;
     float* EPo = R + 4 * ((size_t)V + (size_t)F);
     if (!lak && QUAD && !L.poly_fn)
-        launch_k(k_fp_slak_quad, grid_for(F), kBlock, str, reinterpret_cast<const int4*>(L.ids), L.verts, F, FPo);
+        launch_g<k_fp_slak_quad_g>(grid_for(F), kBlock, str, reinterpret_cast<const int4*>(L.ids), L.verts, F, FPo);
     else if (lak)
-        launch_k(k_fp_seq<QUAD, true>, grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
+        launch_g<k_fp_seq_g<QUAD, true>>(grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
     else
-        launch_k(k_fp_seq<QUAD, false>, grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
+        launch_g<k_fp_seq_g<QUAD, false>>(grid_for(F), kBlock, str, L.ptr, L.ids, L.verts, F, FPo);
     lc.after("k_fp");
     if (lc.conc) lc.fork(1);
     cudaStream_t s_ep = lc.conc ? lc.side[1] : str;
     if (lak)
-        launch_k(k_ep<QUAD, true>, grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        launch_g<k_ep_g<QUAD, true>>(grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
     else
-        launch_k(k_ep<QUAD, false>, grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
+        launch_g<k_ep_g<QUAD, false>>(grid_for(E), kBlock, s_ep, fc, L.ids, s.H, E, L.verts, FPo, EPo);
     lc.after("k_ep");
     const int bnd = L.B > 0;
     if (lak)
-        launch_k(k_vp_lak<QUAD>, grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
+        launch_g<k_vp_lak_g<QUAD>>(grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
                                                         s.eid, bnd, L.verts, FPo, R, compensated);
     else
-        launch_k(k_vp_slak<QUAD>, grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
+        launch_g<k_vp_slak_g<QUAD>>(grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
                                                          L.verts, FPo, R, compensated);
     lc.after("k_vp");
     if (lc.conc) { lc.join(0); lc.join(1); }
@@ -389,7 +389,7 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        launch_k(k_g1<LAK, STATE, PQ, BS, BND, GQ, SG>, grid_for(L.F, BS), BS, str, d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
+        launch_g<k_g1_g<LAK, STATE, PQ, BS, BND, GQ, SG>>(grid_for(L.F, BS), BS, str, d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
             optr, ovals);
     });
     // GQ: k_g1 also writes the vertex points of P's vertices past V2 (and SLAK their slots' edge points)
@@ -399,20 +399,20 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
         // k_gf, k_g2 and k_g3 read only k_g1's records and the level's inputs and
         // write disjoint outputs: with side streams they run side by side
         if (lc.conc) { lc.fork(0); lc.fork(1); }
-        launch_k(k_gf<LAK, STATE>, grid_for(Pl.F), kBlock, lc.conc ? lc.side[0] : str, d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts, comp ? 1 : 0);
+        launch_g<k_gf_g<LAK, STATE>>(grid_for(Pl.F), kBlock, lc.conc ? lc.side[0] : str, d, Pl.ptr, L.ids, L.verts, L.out_state, L.o_verts, comp ? 1 : 0);
         lc.after("k_gf");
         with_block(L.bs[1], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            launch_k(k_g2<LAK, STATE, PQ, BS, BND>, grid_for(L.F, BS), BS, lc.conc ? lc.side[1] : str, d, pf, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
+            launch_g<k_g2_g<LAK, STATE, PQ, BS, BND>>(grid_for(L.F, BS), BS, lc.conc ? lc.side[1] : str, d, pf, L.ids, L.verts, L.in_state, L.out_state, L.o_verts);
         });
         lc.after("k_g2", 1, g2b);
     }
     if (!BND && !SG && L.bulk3) {
-        launch_k(k_g3_bulk<LAK, STATE>, grid_for(nv3 + 1, kBulkBlock), kBulkBlock, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
+        launch_g<k_g3_bulk_g<LAK, STATE>>(grid_for(nv3 + 1, kBulkBlock), kBulkBlock, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3, L.st, L.bulk_polls);
     } else {
         with_block(L.bs[2], [&](auto b) {
             constexpr int BS = decltype(b)::value;
-            launch_k(k_g3<LAK, STATE, BS, BND, SG>, grid_for(nv3 + 1, BS), BS, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3);
+            launch_g<k_g3_g<LAK, STATE, BS, BND, SG>>(grid_for(nv3 + 1, BS), BS, str, d, L.verts, L.in_state, L.out_state, L.slots, L.o_verts, comp ? 1 : 0, nv3);
         });
     }
     // compulsory bytes: the vertex points of its vertices, SLAK the edge points of their slots
@@ -511,7 +511,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
 {
     int64_t nl = 0;
     Lc lc{str, &nl, p->debug, 0};
-    if (p->side[0] && !(p->flags & SLAK_PLAN_TIMING) && !p->debug) {
+    if (p->side[0] && !(p->flags & SLAK_PLAN_TIMING) && !p->debug && !g_record) {
         lc.conc = true;
         for (int k = 0; k < 2; ++k) lc.side[k] = p->side[k];
         for (int k = 0; k < 4; ++k) lc.cev[k] = p->cev[k];
@@ -526,7 +526,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         lc.recs = &p->recs;
         cudaEventRecord(p->ev[0], str);
     }
-    cudaMemsetAsync(p->st, 0, sizeof(DevStatus), str);
+    zero_async(p->st, sizeof(DevStatus), str);
     const bool comp = (p->flags & SLAK_PLAN_COMPENSATED) != 0;
     for (size_t li = 0; li < p->lv.size(); ++li) {
         const Level& L = p->lv[li];
@@ -541,7 +541,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         if (L.quad) launch_rest<true>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
         else launch_rest<false>(L, (int)li, p->scheme, comp, p->s, p->st, lc);
         if (L.export_state && L.B > 0) {     // the edges' boundary ranks
-            launch_k(k_export_bflag, grid_for(L.E), kBlock, str, (int)L.E, p->s.H, p->s.xisb);
+            launch_g<k_export_bflag_g>(grid_for(L.E), kBlock, str, (int)L.E, p->s.H, p->s.xisb);
             lc.after("k_export_bflag");
             int64_t n3 = 0;
             scan_exclusive(p->s.xisb, p->s.xbrank, L.E, p->s.tmp, str, &n3);
@@ -610,7 +610,7 @@ int probe_level0(slak_plan* p, Level& L0, cudaStream_t str, void* given = nullpt
     Lc lc{str, &nl, p->debug, 0};
     cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
     launch_topology_a(L0, 0, p->scheme, s, st, lc);
-    launch_k(k_valence_hist, grid_for(L0.V), kBlock, str, (int)L0.V, s.sptr, st->vhist);
+    launch_g<k_valence_hist_g>(grid_for(L0.V), kBlock, str, (int)L0.V, s.sptr, st->vhist);
     cudaMemcpyAsync(p->h_st, st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
     cudaMemcpyAsync(&p->h_st->nedges, s.eptr + L0.V, sizeof(int), cudaMemcpyDeviceToHost, str);
     e = cudaStreamSynchronize(str);
@@ -1382,17 +1382,22 @@ int slak_mesh_free(slak_mesh* m)
 //
 // Every mesh gets its own plan (so each mesh's numbering and float results are
 // exactly those of slak_subdivide on it alone), but all plans are sized up
-// front, share one device arena per wave and write straight into one batch
-// output buffer.  Within a wave, meshes are dealt round-robin onto parallel
-// streams, so small meshes run concurrently; waves reuse the arena in turn.
-// With SLAK_PLAN_GRAPH the whole batch (every wave, mesh and level) is captured
-// as one CUDA graph whose branches are the per-mesh level chains.
+// front and write straight into one batch output buffer.  Meshes are dealt to
+// kBatchStreams chains, longest predicted time first, each to the chain with
+// the least predicted time so far; a chain runs its meshes one after another
+// (in mesh order, so large and small ones alternate) on its own stream and
+// reuses one slice of the arena sized to its largest mesh.  The chains run
+// concurrently and join once.  Only when the chains' slices do not fit the
+// memory budget does the batch fall back to several such waves, joined in
+// turn.  With SLAK_PLAN_GRAPH the whole batch (every wave, mesh and level) is
+// captured as one CUDA graph whose branches are the chains.
 struct slak_batch {
     int scheme = SLAK_SCHEME_SLAK;
     int flags = 0;
     std::vector<slak_plan*> plans;              // nullptr where the mesh is not refined
     std::vector<slak_mesh> outs;
-    std::vector<std::vector<int64_t>> waves;    // mesh indices per wave
+    std::vector<std::vector<int64_t>> waves;    // mesh indices per wave, in enqueue order
+    std::vector<int> chain;                     // per mesh: its chain (stream) within its wave
     void* out_mem = nullptr;
     void* arena = nullptr;
     size_t out_bytes = 0, arena_bytes = 0;
@@ -1410,11 +1415,35 @@ struct slak_batch {
     int executed = 0;
     bool per_mesh_out = false;                  // outputs allocated per mesh (slak_subdivide_batched)
     std::vector<char> out_given;                // per mesh: arrays handed to the caller
+    // small meshes run in groups: meshes whose plans launch the same kernels
+    // in the same order, each step one grouped launch over all of them
+    struct GroupStep {
+        GroupLaunchFn fn;
+        unsigned grid, block;
+        size_t args_off, bstart_off;            // in gmem
+    };
+    struct Group {
+        std::vector<int64_t> meshes;
+        std::vector<GroupStep> steps;
+        double cost = 0.0;
+    };
+    std::vector<Group> groups;
+    std::vector<char> grouped;                  // per mesh
+    void* gmem = nullptr;                       // device: the groups' argument packs and block offsets
+    std::vector<cudaStream_t> gstreams;
+    std::vector<int> gstream_of;                // per group
+    cudaEvent_t gfork = nullptr;
+    std::vector<cudaEvent_t> gjoin;
 };
 
 namespace {
 
 constexpr int kBatchStreams = 16;
+constexpr int kGroupStreams = 4;
+// meshes refined to fewer quads than this run in groups;
+// SLAK_BATCH_GROUP_QUADS overrides it (0: no groups)
+constexpr int64_t kGroupQuads = int64_t(1) << 19;
+constexpr size_t kGroupSliceBytes = size_t(1) << 30;       // scratch of one group, at most
 
 void batch_free(slak_batch* b)
 {
@@ -1437,6 +1466,10 @@ void batch_free(slak_batch* b)
                 if (m.vals) cudaFree(m.vals);
             }
     if (b->arena) cudaFree(b->arena);
+    if (b->gmem) cudaFree(b->gmem);
+    for (auto s : b->gstreams) cudaStreamDestroy(s);
+    if (b->gfork) cudaEventDestroy(b->gfork);
+    for (auto e : b->gjoin) cudaEventDestroy(e);
     if (b->d_st) cudaFree(b->d_st);
     if (b->h_st) cudaFreeHost(b->h_st);
     delete b;
@@ -1449,17 +1482,44 @@ size_t out_bytes_of(const slak_mesh& o, bool lak)
     return b;
 }
 
+// Predicted device time of one mesh's plan while kBatchStreams chains share
+// the GPU: its levels' refined quads at 1/kBatchStreams of a measured
+// 55 G quads/s, plus the dependent launches' latency (level 0 about 45 us,
+// each later level about 12 us), which concurrency does not divide.
+double batch_cost_us(const slak_plan* p)
+{
+    double quads = 0.0;
+    for (const Level& L : p->lv) quads += (double)L.Fo;
+    return quads * kBatchStreams / 55.0e3 + 45.0 + 12.0 * (double)(p->lv.size() - 1);
+}
+
 int batch_enqueue(slak_batch* b, cudaStream_t str)
 {
     int64_t nl = 0;
+    // the groups, on their own streams beside the chains
+    if (!b->groups.empty()) {
+        cudaEventRecord(b->gfork, str);
+        for (auto gs : b->gstreams) cudaStreamWaitEvent(gs, b->gfork, 0);
+        char* gm = static_cast<char*>(b->gmem);
+        for (size_t g = 0; g < b->groups.size(); ++g) {
+            const auto& G = b->groups[g];
+            cudaStream_t gs = b->gstreams[b->gstream_of[g]];
+            for (const auto& st : G.steps) {
+                st.fn(gm + st.args_off, reinterpret_cast<const unsigned*>(gm + st.bstart_off), (int)G.meshes.size(),
+                      st.grid, st.block, gs);
+                ++nl;
+            }
+        }
+    }
     for (size_t w = 0; w < b->waves.size(); ++w) {
         const auto& wave = b->waves[w];
-        const int nb = (int)std::min<size_t>(kBatchStreams, wave.size());
+        int nb = 0;
+        for (int64_t i : wave) nb = std::max(nb, b->chain[i] + 1);
         cudaEventRecord(b->fork[w], str);
         for (int k = 0; k < nb; ++k) cudaStreamWaitEvent(b->streams[k], b->fork[w], 0);
         for (size_t j = 0; j < wave.size(); ++j) {
             slak_plan* p = b->plans[wave[j]];
-            const int k = (int)(j % nb);
+            const int k = b->chain[wave[j]];
             if (!b->side.empty()) {
                 p->side[0] = b->side[2 * k];
                 p->side[1] = b->side[2 * k + 1];
@@ -1475,7 +1535,149 @@ int batch_enqueue(slak_batch* b, cudaStream_t str)
             cudaStreamWaitEvent(str, b->join[w * kBatchStreams + k], 0);
         }
     }
+    if (!b->groups.empty())
+        for (size_t k = 0; k < b->gstreams.size(); ++k) {
+            cudaEventRecord(b->gjoin[k], b->gstreams[k]);
+            cudaStreamWaitEvent(str, b->gjoin[k], 0);
+        }
     b->launches = nl;
+    return cuda_status(cudaGetLastError());
+}
+
+// Records the launches one execution of plan p makes, without launching.
+int record_plan(slak_plan* p, std::vector<RecLaunch>& r, cudaStream_t str)
+{
+    g_record = &r;
+    const int rc = enqueue_all(p, str);
+    g_record = nullptr;
+    return rc;
+}
+
+// The groups of small meshes, before any memory exists.  Each candidate's
+// plan is wired to null scratch and its launch sequence recorded (the
+// sequence does not depend on addresses); meshes with the same sequence form
+// a kind, and each kind is cut into groups of at most `slice` bytes of
+// scratch.  Groups go to kGroupStreams streams (longest predicted first, to
+// the least loaded); a stream's groups run one after another in one region
+// of the arena sized to its largest group.  Sets b->groups, b->gstream_of,
+// b->grouped, each grouped mesh's offset in `aoff` (from the start of the
+// groups' part of the arena) and returns that part's size.
+size_t batch_plan_groups(slak_batch* b, const std::vector<int64_t>& cand, const std::vector<size_t>& ab,
+                         const std::vector<double>& cost, size_t slice, std::vector<size_t>& aoff, cudaStream_t str,
+                         int* rc)
+{
+    std::map<std::vector<std::pair<uintptr_t, unsigned>>, std::vector<int64_t>> kinds;
+    for (int64_t i : cand) {
+        slak_plan* p = b->plans[i];
+        if (ab[i] > slice) continue;
+        p->arena = nullptr;
+        Carver dry(nullptr);
+        plan_carve(p, dry);
+        p->st = nullptr;
+        p->out = b->outs[i];
+        plan_wire(p);
+        std::vector<RecLaunch> r;
+        *rc = record_plan(p, r, str);
+        if (*rc != SLAK_OK) return 0;
+        std::vector<std::pair<uintptr_t, unsigned>> key;
+        for (const auto& x : r) key.emplace_back(reinterpret_cast<uintptr_t>(x.fn), x.block);
+        kinds[key].push_back(i);
+    }
+    std::vector<size_t> gbytes;
+    for (auto& kv : kinds) {
+        size_t used = slice;
+        for (int64_t i : kv.second) {
+            if (used + ab[i] > slice) {
+                b->groups.emplace_back();
+                gbytes.push_back(0);
+                used = 0;
+            }
+            slak_batch::Group& G = b->groups.back();
+            aoff[i] = used;                 // within the group, for now
+            G.meshes.push_back(i);
+            G.cost += cost[i];
+            used += ab[i];
+            gbytes.back() = used;
+            b->grouped[i] = 1;
+        }
+    }
+    const int ns = (int)std::min<size_t>(kGroupStreams, b->groups.size());
+    if (ns == 0) return 0;
+    std::vector<size_t> ord(b->groups.size());
+    for (size_t g = 0; g < ord.size(); ++g) ord[g] = g;
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return b->groups[x].cost > b->groups[y].cost; });
+    std::vector<double> load(ns, 0.0);
+    std::vector<size_t> region(ns, 0);
+    b->gstream_of.assign(b->groups.size(), 0);
+    for (size_t g : ord) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        b->gstream_of[g] = k;
+        load[k] += b->groups[g].cost;
+        region[k] = std::max(region[k], gbytes[g]);
+    }
+    std::vector<size_t> base(ns, 0);
+    size_t tot = 0;
+    for (int k = 0; k < ns; ++k) { base[k] = tot; tot += region[k]; }
+    for (size_t g = 0; g < b->groups.size(); ++g)
+        for (int64_t i : b->groups[g].meshes) aoff[i] += base[b->gstream_of[g]];
+    return tot;
+}
+
+// Records every grouped mesh's launches again, now with its real scratch and
+// outputs, and uploads each group step's argument packs and block offsets.
+int batch_upload_groups(slak_batch* b, cudaStream_t str)
+{
+    if (b->groups.empty()) return SLAK_OK;
+    std::vector<std::vector<RecLaunch>> rec(b->plans.size());
+    for (const auto& G : b->groups)
+        for (int64_t i : G.meshes) {
+            const int rc = record_plan(b->plans[i], rec[i], str);
+            if (rc != SLAK_OK) return rc;
+        }
+    size_t off = 0;
+    for (auto& G : b->groups) {
+        const auto& r0 = rec[G.meshes[0]];
+        const size_t nm = G.meshes.size();
+        for (size_t j = 0; j < r0.size(); ++j) {
+            slak_batch::GroupStep st{r0[j].fn, 0u, r0[j].block, off, 0};
+            off += align_up(nm * r0[j].pack.size());
+            st.bstart_off = off;
+            off += align_up(sizeof(unsigned) * (nm + 1));
+            G.steps.push_back(st);
+        }
+    }
+    std::vector<unsigned char> hb(off, 0);
+    for (auto& G : b->groups) {
+        const size_t nm = G.meshes.size();
+        for (size_t j = 0; j < G.steps.size(); ++j) {
+            auto& st = G.steps[j];
+            unsigned* bs = reinterpret_cast<unsigned*>(hb.data() + st.bstart_off);
+            uint64_t tot = 0;
+            for (size_t m = 0; m < nm; ++m) {
+                const auto& rm = rec[G.meshes[m]];
+                // the same launcher (kernel and argument types) in every mesh of the group
+                if (rm.size() != G.steps.size() || rm[j].fn != st.fn || rm[j].block != st.block) {
+                    g_detail = "grouped launch: launch sequences differ";
+                    return SLAK_ERR_INVALID_ARG;
+                }
+                std::memcpy(hb.data() + st.args_off + m * rm[j].pack.size(), rm[j].pack.data(), rm[j].pack.size());
+                bs[m] = (unsigned)tot;
+                tot += rm[j].grid;
+            }
+            bs[nm] = (unsigned)tot;
+            if (tot >= (uint64_t(1) << 31)) return SLAK_ERR_UNSUPPORTED;
+            st.grid = (unsigned)tot;
+        }
+    }
+    cudaError_t ce = cudaMalloc(&b->gmem, off);
+    if (ce == cudaSuccess) ce = cudaMemcpy(b->gmem, hb.data(), off, cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return cuda_status(ce);
+    const int ns = *std::max_element(b->gstream_of.begin(), b->gstream_of.end()) + 1;
+    b->gstreams.resize(ns);
+    for (auto& gs : b->gstreams) cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&b->gfork, cudaEventDisableTiming);
+    b->gjoin.resize(ns);
+    for (auto& e : b->gjoin) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1544,7 +1746,7 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
                 if (!p) continue;
                 cudaMemsetAsync(st, 0, sizeof(DevStatus), str);
                 launch_topology_a(p->lv[0], 0, scheme, sc, st, lc);
-                launch_k(k_valence_hist, grid_for(p->lv[0].V), kBlock, str, (int)p->lv[0].V, sc.sptr, st->vhist);
+                launch_g<k_valence_hist_g>(grid_for(p->lv[0].V), kBlock, str, (int)p->lv[0].V, sc.sptr, st->vhist);
                 cudaMemcpyAsync(&b->h_st[i], st, sizeof(DevStatus), cudaMemcpyDeviceToHost, str);
                 cudaMemcpyAsync(&b->h_st[i].nedges, sc.eptr + p->lv[0].V, sizeof(int), cudaMemcpyDeviceToHost, str);
             }
@@ -1568,8 +1770,11 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
             else rc = plan_levels(p);
         }
     }
-    // memory: every mesh's output in one buffer; waves of plans sharing one arena
-    std::vector<size_t> ab(count, 0), ob(count, 0);
+    // memory: every mesh's output in one buffer; chains of plans, each chain
+    // reusing one arena slice
+    std::vector<size_t> ab(count, 0), ob(count, 0), aoff(count, 0);
+    std::vector<double> cost(count, 0.0);
+    b->chain.assign(count, 0);
     size_t total_out = 0;
     for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
         slak_plan* p = b->plans[i];
@@ -1580,6 +1785,7 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
         b->outs[i] = plan_output_shape(p);
         ob[i] = out_bytes_of(b->outs[i], scheme == SLAK_SCHEME_LAK);
         total_out += ob[i];
+        cost[i] = batch_cost_us(p);
     }
     if (rc == SLAK_OK) {
         size_t freeb = 0, totalb = 0;
@@ -1590,24 +1796,82 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
         size_t cap = size_t(24) << 30;
         if (const char* wb = std::getenv("SLAK_BATCH_WAVE_BYTES")) cap = (size_t)std::strtoull(wb, nullptr, 10);
         if (budget > cap) budget = cap;
-        // greedy waves in mesh order; a mesh above the wave cap (but within
-        // free memory) runs in a wave of its own
-        const size_t hard = rc == SLAK_OK ? (freeb - total_out - margin) * 3 / 4 : 0;
-        std::vector<int64_t> cur;
-        size_t cur_b = 0;
-        for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
-            if (!b->plans[i]) continue;
-            if (ab[i] > hard) { g_detail = "mesh " + std::to_string(i) + " needs more scratch than is free"; rc = SLAK_ERR_OOM; break; }
-            if (cur_b + ab[i] > budget && !cur.empty()) {
-                b->waves.push_back(cur);
-                b->arena_bytes = std::max(b->arena_bytes, cur_b);
-                cur.clear();
-                cur_b = 0;
+        // small meshes run in groups (kinds of identical launch sequences cut
+        // into groups of at most `slice` bytes of scratch); the groups' part
+        // of the arena takes at most half the budget
+        b->grouped.assign(count, 0);
+        int64_t gq = kGroupQuads;
+        if (const char* e = std::getenv("SLAK_BATCH_GROUP_QUADS")) gq = std::atoll(e);
+        size_t gbytes = 0;
+        if (rc == SLAK_OK && gq > 0 && !(flags & SLAK_PLAN_TIMING)) {
+            std::vector<int64_t> cand;
+            for (int64_t i = 0; i < count; ++i) {
+                slak_plan* p = b->plans[i];
+                if (p && !p->debug && p->lv.back().Fo < gq) cand.push_back(i);
             }
-            cur.push_back(i);
-            cur_b += ab[i];
+            const size_t slice = std::min(kGroupSliceBytes, budget / (2 * kGroupStreams));
+            gbytes = batch_plan_groups(b, cand, ab, cost, slice, aoff, str, &rc);
         }
-        if (!cur.empty()) { b->waves.push_back(cur); b->arena_bytes = std::max(b->arena_bytes, cur_b); }
+        budget -= std::min(budget, gbytes);
+        // meshes by predicted time, longest first; each goes to the chain with
+        // the least predicted time so far, unless the chains' slices would
+        // outgrow the budget, which closes the wave.  A mesh above the budget
+        // (but within free memory) runs in a wave of its own.
+        const size_t hard = rc == SLAK_OK ? (freeb - total_out - margin) * 3 / 4 : 0;
+        std::vector<int64_t> order;
+        for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
+            if (!b->plans[i] || b->grouped[i]) continue;
+            if (ab[i] > hard) { g_detail = "mesh " + std::to_string(i) + " needs more scratch than is free"; rc = SLAK_ERR_OOM; break; }
+            order.push_back(i);
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return cost[x] > cost[y]; });
+        std::vector<std::vector<int64_t>> chains(kBatchStreams);
+        std::vector<size_t> slice(kBatchStreams, 0);
+        std::vector<double> load(kBatchStreams, 0.0);
+        size_t used = 0;
+        auto close_wave = [&]() {
+            size_t off = 0;
+            std::vector<int64_t> wave;
+            for (int k = 0; k < kBatchStreams; ++k) {
+                std::sort(chains[k].begin(), chains[k].end());
+                for (int64_t i : chains[k]) aoff[i] = off;
+                off += slice[k];
+            }
+            // enqueue order: the chains' first meshes, then their second ones, ...
+            for (size_t j = 0;; ++j) {
+                bool any = false;
+                for (int k = 0; k < kBatchStreams; ++k)
+                    if (j < chains[k].size()) { wave.push_back(chains[k][j]); any = true; }
+                if (!any) break;
+            }
+            if (!wave.empty()) b->waves.push_back(wave);
+            b->arena_bytes = std::max(b->arena_bytes, off);
+            for (int k = 0; k < kBatchStreams; ++k) { chains[k].clear(); slice[k] = 0; load[k] = 0.0; }
+            used = 0;
+        };
+        for (int64_t i : order) {
+            int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            size_t grow = ab[i] > slice[k] ? ab[i] - slice[k] : 0;
+            if (used + grow > budget && used > 0) {
+                // the chain whose slice already holds it, else a new wave
+                int fit = -1;
+                for (int c = 0; c < kBatchStreams; ++c)
+                    if (slice[c] >= ab[i] && (fit < 0 || load[c] < load[fit])) fit = c;
+                if (fit >= 0) { k = fit; grow = 0; }
+                else { close_wave(); k = 0; grow = ab[i]; }
+            }
+            chains[k].push_back(i);
+            b->chain[i] = k;
+            slice[k] += grow;
+            used += grow;
+            load[k] += cost[i];
+        }
+        close_wave();
+        // the groups' part after the chains' region
+        const size_t goff = b->arena_bytes;
+        for (int64_t i = 0; i < count; ++i)
+            if (b->grouped[i]) aoff[i] += goff;
+        b->arena_bytes = goff + gbytes;
     }
     if (rc == SLAK_OK && total_out) {
         if (!b->per_mesh_out) ce = cudaMalloc(&b->out_mem, total_out);
@@ -1640,18 +1904,15 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
                 m.vals = reinterpret_cast<int*>(o); o += align_up(sizeof(int) * (size_t)m.nnz);
             }
         }
-        for (const auto& wave : b->waves) {
-            size_t off = 0;
-            for (int64_t i : wave) {
-                slak_plan* p = b->plans[i];
-                p->arena = static_cast<char*>(b->arena) + off;
-                Carver cv(static_cast<char*>(p->arena));
-                plan_carve(p, cv);
-                p->st = b->d_st + i;           // the arena is reused by later waves
-                off += ab[i];
-                p->out = b->outs[i];
-                plan_wire(p);
-            }
+        for (int64_t i = 0; i < count; ++i) {
+            slak_plan* p = b->plans[i];
+            if (!p) continue;
+            p->arena = static_cast<char*>(b->arena) + aoff[i];
+            Carver cv(static_cast<char*>(p->arena));
+            plan_carve(p, cv);
+            p->st = b->d_st + i;               // a chain's slice is reused by its later meshes
+            p->out = b->outs[i];
+            plan_wire(p);
         }
         b->fork.resize(b->waves.size());
         b->join.resize(b->waves.size() * kBatchStreams);
@@ -1668,12 +1929,15 @@ static int batch_create_impl(const slak_mesh* meshes, const int* levels, int64_t
     }
     // launch shapes: cached choices, or (SLAK_PLAN_AUTOTUNE) measured on the
     // first mesh of each key, alone on `stream`, before any batch execution
+    // (grouped meshes keep the default shapes, so that more of them share a
+    // launch sequence)
     for (int64_t i = 0; i < count && rc == SLAK_OK; ++i) {
         slak_plan* p = b->plans[i];
-        if (!p) continue;
+        if (!p || b->grouped[i]) continue;
         if (flags & SLAK_PLAN_AUTOTUNE) rc = plan_autotune(p, str);
         else apply_tuning(p);
     }
+    if (rc == SLAK_OK) rc = batch_upload_groups(b, str);
     if (rc != SLAK_OK) { batch_free(b); return rc; }
     *out_batch = b;
     return SLAK_OK;
@@ -1762,6 +2026,8 @@ int slak_batch_output(const slak_batch* b, int64_t index, slak_mesh* rmesh)
 }
 
 int slak_batch_num_waves(const slak_batch* b) { return b ? (int)b->waves.size() : 0; }
+
+int slak_batch_num_groups(const slak_batch* b) { return b ? (int)b->groups.size() : 0; }
 
 int64_t slak_batch_launches(const slak_batch* b) { return b ? b->launches : 0; }
 

@@ -1,6 +1,6 @@
 """Batched refinement: every mesh's output equals slak_subdivide on that mesh
-alone, bit for bit, across mixed mesh kinds, level counts, waves and graph
-replay."""
+alone, bit for bit, across mixed mesh kinds, level counts, grouped launches,
+chains, waves and graph replay."""
 import os
 
 import numpy as np
@@ -27,23 +27,37 @@ def _bits(a):
     return np.asarray(a, np.float32).view(np.uint32)
 
 
+# mode: (graph, SLAK_BATCH_GROUP_QUADS, SLAK_BATCH_WAVE_BYTES); these meshes
+# refine to at most 768k quads, so a bound of 4M groups all of them
+MODES = {"grouped": (False, "4000000", None), "grouped-graph": (True, "4000000", None),
+         "chains": (False, "0", None), "chains-graph": (True, "0", None),
+         "mixed-graph": (True, "20000", None), "waves": (False, "0", "1")}
+
+
 @pytest.mark.parametrize("scheme", [SLAK, LAK])
-@pytest.mark.parametrize("mode", ["eager", "graph", "waves"])
+@pytest.mark.parametrize("mode", list(MODES))
 def test_batch_matches_single(scheme, mode, monkeypatch):
     import torch
     items = _meshes()
     if scheme == LAK:
         items = [(m if m.ptr is not None else m.with_quad_ptr(), l) for m, l in items]
-    if mode == "waves":
-        monkeypatch.setenv("SLAK_BATCH_WAVE_BYTES", str(8 << 20))
+    graph, gq, wb = MODES[mode]
+    if gq is not None:
+        monkeypatch.setenv("SLAK_BATCH_GROUP_QUADS", gq)
+    if wb is not None:                         # a 1-byte budget: every chain reuses its slice
+        monkeypatch.setenv("SLAK_BATCH_WAVE_BYTES", wb)
     dms = [api.DeviceMesh.from_host(m) for m, _ in items]
     s = torch.cuda.Stream()
-    flags = api._abi.PLAN_GRAPH if mode == "graph" else 0
+    flags = api._abi.PLAN_GRAPH if graph else 0
     with torch.cuda.stream(s):
         b = api.Batch(dms, [l for _, l in items], scheme, flags, stream=s)
-        if mode == "waves":
-            assert b.waves > 1
-        for _ in range(2 if mode == "graph" else 1):
+        if mode.startswith("grouped"):
+            assert b.groups >= 1 and b.waves == 0
+        elif mode.startswith("chains") or mode == "waves":
+            assert b.groups == 0 and b.waves >= 1
+        else:
+            assert b.groups >= 1 and b.waves >= 1
+        for _ in range(2 if graph else 1):
             b.execute(s)
             b.check(s)
         outs = [b.output(i) for i in range(len(items))]
@@ -62,6 +76,27 @@ def test_batch_matches_single(scheme, mode, monkeypatch):
     b.close()
 
 
+def test_groups_cut_launches(monkeypatch):
+    """Grouped launches: one launch per step of each group instead of one per
+    step of each mesh."""
+    import torch
+    items = _meshes()
+    dms = [api.DeviceMesh.from_host(m) for m, _ in items]
+    s = torch.cuda.Stream()
+    counts = {}
+    with torch.cuda.stream(s):
+        for gq in ("0", "4000000"):
+            monkeypatch.setenv("SLAK_BATCH_GROUP_QUADS", gq)
+            b = api.Batch(dms, [l for _, l in items], SLAK, 0, stream=s)
+            b.execute(s)
+            b.check(s)
+            counts[gq] = (b.launches, b.groups)
+            b.close()
+    (chained, _), (grouped, ngroups) = counts["0"], counts["4000000"]
+    assert 1 <= ngroups < len(items)
+    assert grouped * 2 < chained               # 29 meshes of many kinds: 174 against 510 on B200
+
+
 @pytest.mark.parametrize("scheme", [SLAK, LAK])
 @pytest.mark.parametrize("waves", [False, True])
 def test_subdivide_batched_one_call(scheme, waves, monkeypatch):
@@ -71,8 +106,9 @@ def test_subdivide_batched_one_call(scheme, waves, monkeypatch):
     items = _meshes()
     if scheme == LAK:
         items = [(m if m.ptr is not None else m.with_quad_ptr(), l) for m, l in items]
-    if waves:
-        monkeypatch.setenv("SLAK_BATCH_WAVE_BYTES", str(8 << 20))
+    if waves:                                  # chains only, on a 1-byte budget
+        monkeypatch.setenv("SLAK_BATCH_GROUP_QUADS", "0")
+        monkeypatch.setenv("SLAK_BATCH_WAVE_BYTES", "1")
     dms = [api.DeviceMesh.from_host(m) for m, _ in items]
     outs = api.subdivide_batched(dms, [l for _, l in items], scheme)
     torch.cuda.synchronize()
