@@ -11,6 +11,7 @@
 #include <type_traits>
 #include <utility>
 #include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace slak {
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(kBlock) k_zero(int* __restrict__ p, int64_t n)
 }
 struct k_zero_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const { k_zero_body(bx, a...); }
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const { k_zero_body(bx, a...); }
     static constexpr auto kernel() { return &k_zero; }
 };
 

@@ -46,6 +46,11 @@ constexpr bool kFaceSumShfl = true;       // comparison builds: the face sums by
 #else
 constexpr bool kFaceSumShfl = false;
 #endif
+#ifdef SLAK_NO_TMA_STORE
+constexpr bool kTmaQuadStore = false;     // comparison builds: refined quads by coalesced stores
+#else
+constexpr bool kTmaQuadStore = true;
+#endif
 
 __device__ __forceinline__ int qnext(int x) { return (x & ~3) | ((x + 1) & 3); }
 __device__ __forceinline__ int qprev(int x) { return (x & ~3) | ((x + 3) & 3); }
@@ -466,9 +471,9 @@ __device__ __forceinline__ int sg_sptr(const FastDims& d, const int* __restrict_
 // refined quads of its span with consecutive threads (coalesced).
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
 __device__ __forceinline__ void k_g1_body(const unsigned bx_, FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                                              const float* __restrict__ P, QState p, QState c,
-                                                              int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
-                                                              int* __restrict__ optr, int4* __restrict__ ovals)
+                                          const float* __restrict__ P, QState p, QState c,
+                                          int4* __restrict__ out_ids, const CUtensorMap& otm, float* __restrict__ R,
+                                          SlotScratch z, int* __restrict__ optr, int4* __restrict__ ovals)
 {
     const int x0 = bx_ * blockDim.x;
     const int x = x0 + threadIdx.x;
@@ -574,6 +579,28 @@ __device__ __forceinline__ void k_g1_body(const unsigned bx_, FastDims d, Faces<
             int4* dst = out_ids + 4 * (int64_t)x;
             st8_cs(dst, make_int4(Q.x, VFc + e0, fpid, VFc + e3), make_int4(Q.y, VFc + e1, fpid, VFc + e0));
             st8_cs(dst + 2, make_int4(Q.z, VFc + e2, fpid, VFc + e1), make_int4(Q.w, VFc + e3, fpid, VFc + e2));
+        }
+    } else if constexpr (kTmaQuadStore && BS <= 256) {
+        // the block's refined quads (row t = thread t's 64 bytes) staged in
+        // shared memory in the tensor map's 64-byte swizzle (16-byte chunk k
+        // of row t at chunk k ^ (t/2 mod 4): a warp's stores of chunk k fall on
+        // all 32 banks), then one TMA tensor store of the block's rows; rows
+        // past N1 are clipped by the map.  Replaces the shared-memory round
+        // trip and the coalesced stores of the staged layout below.
+        __shared__ __align__(1024) int4 sq[4 * BS];
+        const int t = threadIdx.x, sw = (t >> 1) & 3;
+        sq[4 * t + (0 ^ sw)] = make_int4(Q.x, VFc + e0, fpid, VFc + e3);
+        sq[4 * t + (1 ^ sw)] = make_int4(Q.y, VFc + e1, fpid, VFc + e0);
+        sq[4 * t + (2 ^ sw)] = make_int4(Q.z, VFc + e2, fpid, VFc + e1);
+        sq[4 * t + (3 ^ sw)] = make_int4(Q.w, VFc + e3, fpid, VFc + e2);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                         :: "l"(reinterpret_cast<uint64_t>(&otm)), "r"(0), "r"(x0),
+                            "r"((uint32_t)__cvta_generic_to_shared(sq))
+                         : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
     } else {
         // refined quad k of thread t at sq[k * (BS + 2) + t]: the stores
@@ -742,20 +769,26 @@ __device__ __forceinline__ void k_g1_body(const unsigned bx_, FastDims d, Faces<
         }
         if (x == 0) optr[d.N] = 4 * d.N;
     }
+    if constexpr (!STATE && kTmaQuadStore && BS <= 256) {
+        // the tensor store has read the staging buffer and its writes are done
+        if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
 }
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
 __global__ void __launch_bounds__(BS, (GQ ? 768 : 1024) / BS) k_g1(FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
                                                                    const float* __restrict__ P, QState p, QState c,
-                                                                   int4* __restrict__ out_ids, float* __restrict__ R, SlotScratch z,
+                                                                   int4* __restrict__ out_ids,
+                                                                   const __grid_constant__ CUtensorMap otm,
+                                                                   float* __restrict__ R, SlotScratch z,
                                                                    int* __restrict__ optr, int4* __restrict__ ovals)
 {
     griddep_enter();
-    k_g1_body<LAK, STATE, PQ, BS, BND, GQ, SG>(blockIdx.x, d, pf, ids, P, p, c, out_ids, R, z, optr, ovals);
+    k_g1_body<LAK, STATE, PQ, BS, BND, GQ, SG>(blockIdx.x, d, pf, ids, P, p, c, out_ids, otm, R, z, optr, ovals);
 }
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false, bool GQ = false, bool SG = false>
 struct k_g1_g {
     static constexpr int kBounds = 2, kMaxT = BS, kMinB = (GQ ? 768 : 1024) / BS;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_g1_body<LAK, STATE, PQ, BS, BND, GQ, SG>(bx, a...);
     }
@@ -906,7 +939,7 @@ __global__ void __launch_bounds__(kBlock) k_gf(FastDims d, const int* __restrict
 template <bool LAK, bool STATE>
 struct k_gf_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_gf_body<LAK, STATE>(bx, a...);
     }
@@ -974,7 +1007,7 @@ __global__ void __launch_bounds__(BS) k_g2(FastDims d, Faces<PQ> pf, const int* 
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 struct k_g2_g {
     static constexpr int kBounds = 1, kMaxT = BS, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_g2_body<LAK, STATE, PQ, BS, BND>(bx, a...);
     }
@@ -1287,7 +1320,7 @@ __global__ void __launch_bounds__(BS) k_g3(FastDims d, const float* __restrict__
 template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
 struct k_g3_g {
     static constexpr int kBounds = 1, kMaxT = BS, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_g3_body<LAK, STATE, BS, BND, SG>(bx, a...);
     }
@@ -1401,7 +1434,7 @@ __global__ void __launch_bounds__(kBulkBlock) k_g3_bulk(FastDims d, const float*
 template <bool LAK, bool STATE>
 struct k_g3_bulk_g {
     static constexpr int kBounds = 1, kMaxT = kBulkBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_g3_bulk_body<LAK, STATE>(bx, a...);
     }
@@ -1425,7 +1458,7 @@ __global__ void k_export_bflag(int E, const int2* __restrict__ H, int* __restric
 }
 struct k_export_bflag_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_export_bflag_body(bx, a...);
     }

@@ -54,7 +54,7 @@ __global__ void k_face_map_valence(const int* __restrict__ ptr, const int* __res
 }
 struct k_face_map_valence_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_face_map_valence_body(bx, a...);
     }
@@ -76,7 +76,7 @@ __global__ void k_valence(const int* __restrict__ ids, int N, int V, int* __rest
 }
 struct k_valence_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_valence_body(bx, a...);
     }
@@ -102,7 +102,7 @@ __global__ void k_valence_hist(int V, const int* __restrict__ sptr, int* __restr
 }
 struct k_valence_hist_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_valence_hist_body(bx, a...);
     }
@@ -132,7 +132,7 @@ __global__ void k_bucket(const int* __restrict__ ids, int N, int V, const int* _
 }
 struct k_bucket_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_bucket_body(bx, a...);
     }
@@ -206,7 +206,7 @@ __global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, cons
 template <bool QUAD>
 struct k_vsort_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_vsort_body<QUAD>(bx, a...);
     }
@@ -345,7 +345,7 @@ __global__ void k_edges(int V, const int* __restrict__ sptr, const int* __restri
 template <bool LAK>
 struct k_edges_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_edges_body<LAK>(bx, a...);
     }
@@ -390,7 +390,7 @@ __global__ void k_eids_slak(int V, const int* __restrict__ sptr, const int* __re
 }
 struct k_eids_slak_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_eids_slak_body(bx, a...);
     }
@@ -532,7 +532,7 @@ __global__ void k_eids_lak(int V, const int* __restrict__ sptr, const int* __res
 }
 struct k_eids_lak_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_eids_lak_body(bx, a...);
     }
@@ -576,7 +576,7 @@ __global__ void k_refine(Faces<QUAD> fc, const int* __restrict__ ids, const int*
 template <bool QUAD, bool LAK>
 struct k_refine_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_refine_body<QUAD, LAK>(bx, a...);
     }
@@ -604,7 +604,7 @@ __global__ void k_fp_slak_quad(const int4* __restrict__ ids4, const float* __res
 }
 struct k_fp_slak_quad_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_fp_slak_quad_body(bx, a...);
     }
@@ -637,7 +637,7 @@ __global__ void k_fp_seq(const int* __restrict__ ptr, const int* __restrict__ id
 template <bool QUAD, bool LAK>
 struct k_fp_seq_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_fp_seq_body<QUAD, LAK>(bx, a...);
     }
@@ -686,7 +686,7 @@ __global__ void k_ep(Faces<QUAD> fc, const int* __restrict__ ids, const int2* __
 template <bool QUAD, bool LAK>
 struct k_ep_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_ep_body<QUAD, LAK>(bx, a...);
     }
@@ -812,7 +812,7 @@ __global__ void k_vp_slak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, c
 template <bool QUAD>
 struct k_vp_slak_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_vp_slak_body<QUAD>(bx, a...);
     }
@@ -988,7 +988,7 @@ __global__ void k_vp_lak(Faces<QUAD> fc, int V, const int* __restrict__ sptr, co
 template <bool QUAD>
 struct k_vp_lak_g {
     static constexpr int kBounds = 0, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_vp_lak_body<QUAD>(bx, a...);
     }

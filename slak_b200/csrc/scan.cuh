@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_reduce(const int* __restrict__ 
 }
 struct k_scan_reduce_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_scan_reduce_body(bx, a...);
     }
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_tiles(int* __restrict__ tsum, i
 }
 struct k_scan_tiles_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_scan_tiles_body(bx, a...);
     }
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_final(const int* __restrict__ i
 }
 struct k_scan_final_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_scan_final_body(bx, a...);
     }
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_final_small(const int* __restri
 }
 struct k_scan_final_small_g {
     static constexpr int kBounds = 1, kMaxT = kBlock, kMinB = 0;
-    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, A... a) const
+    template <class... A> __device__ __forceinline__ void operator()(unsigned bx, const A&... a) const
     {
         k_scan_final_small_body(bx, a...);
     }

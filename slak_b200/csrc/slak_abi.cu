@@ -21,6 +21,7 @@
 #include <cmath>
 #include <map>
 #include <type_traits>
+#include <cudaTypedefs.h>
 
 #include "common.cuh"
 #include "general.cuh"
@@ -371,6 +372,37 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     if (lc.conc) { lc.join(0); lc.join(1); }
 }
 
+// The tensor map of a level's refined quads for k_g1's tensor store: `rows`
+// rows of 16 int32 (thread x's four quads at out + 16 x), boxes of `bs` rows,
+// 64-byte swizzle (the layout k_g1 stages them in).  A null `out` (a launch
+// sequence recorded before any memory exists) leaves the map zeroed.
+bool quad_store_map(CUtensorMap& m, int* out, int64_t rows, int bs)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    if (out == nullptr) return true;
+    if (enc == nullptr || rows < 1) {
+        g_detail = "cuTensorMapEncodeTiled unavailable";
+        return false;
+    }
+    const cuuint64_t dims[2] = {16, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {64};
+    const cuuint32_t box[2] = {16, (cuuint32_t)bs};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, out, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) g_detail = "cuTensorMapEncodeTiled: error " + std::to_string((int)r);
+    return r == CUDA_SUCCESS;
+}
+
 // One fast level: C = L (refined from its parent level Pl, whose state is
 // L.in_state).  BND: Pl has a boundary (quad faces only).
 template <bool LAK, bool STATE, bool PQ, bool BND, bool GQ = false, bool SG = false>
@@ -387,11 +419,21 @@ void launch_fast_t(const Level& Pl, const Level& L, Faces<PQ> pf, bool comp, Lc&
     // LAK's last level: the refined ptr / vals come from k_g1 too
     int* optr = LAK && !STATE ? L.o_ptr : nullptr;
     int4* ovals = LAK && !STATE ? reinterpret_cast<int4*>(L.o_vals) : nullptr;
+    bool mapped = true;
     with_block(L.bs[0], [&](auto b) {
         constexpr int BS = decltype(b)::value;
-        launch_g<k_g1_g<LAK, STATE, PQ, BS, BND, GQ, SG>>(grid_for(L.F, BS), BS, str, d, pf, L.ids, L.verts, L.in_state, L.out_state, reinterpret_cast<int4*>(L.o_ids), L.o_verts, L.slots,
-            optr, ovals);
+        CUtensorMap otm;
+        std::memset(&otm, 0, sizeof otm);
+        if constexpr (!STATE && kTmaQuadStore && BS <= 256) mapped = quad_store_map(otm, L.o_ids, Pl.N, BS);
+        if (!mapped) return;            // nothing of the level is launched
+        launch_g<k_g1_g<LAK, STATE, PQ, BS, BND, GQ, SG>>(grid_for(L.F, BS), BS, str, d, pf, L.ids, L.verts, L.in_state,
+                                                          L.out_state, reinterpret_cast<int4*>(L.o_ids), otm, L.o_verts,
+                                                          L.slots, optr, ovals);
     });
+    if (!mapped) {
+        if (!lc.err) lc.err = SLAK_ERR_CUDA;
+        return;
+    }
     // GQ: k_g1 also writes the vertex points of P's vertices past V2 (and SLAK their slots' edge points)
     const int64_t gqb = GQ ? 16 * (Pl.V - L.gV) + (LAK ? 0 : 16 * (L.F - L.gN)) : 0;
     lc.after("k_g1", 1, (PQ ? g1b + g2b : g1b) + (optr ? 4 * (L.N + 1) + 16 * L.N : 0) + gqb);
@@ -533,6 +575,7 @@ int enqueue_all(slak_plan* p, cudaStream_t str)
         lc.level = (int)li;
         if (L.fast) {
             launch_fast(p->lv[li - 1], L, p->s.cface, p->scheme, comp, lc);
+            if (lc.err) break;          // a level that could not be launched stops the plan
             if ((int)li < p->crease_levels) launch_creases(p, (int)li, lc);
             continue;
         }
