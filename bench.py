@@ -45,7 +45,7 @@ HBM_FALLBACK_GBS = 6650.0
 # (profiles/k_g1_k_g3_last_level_mixed512_slak.txt: k_g1 of the last level,
 # SLAK, per quad of the level it refines, this build); times the units of the
 # bench's launch.
-TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 174.53}
+TRAFFIC_PER_UNIT = {("k_g1", "slak", "last"): 174.88}
 # B200 HBM3e datasheet bandwidth (DGX figure), reported beside the measured peak
 HBM_NOMINAL_GBS = 8000.0
 
