@@ -833,8 +833,8 @@ __device__ __noinline__ float4 face_vertex_compensated(const int* __restrict__ i
 // are quads.  Same formulas and order, with n = k.
 template <bool LAK, bool STATE>
 __device__ __forceinline__ void k_gf_body(const unsigned bx_, FastDims d, const int* __restrict__ pptr, const int* __restrict__ ids,
-                                                              const float* __restrict__ P, QState c, float* __restrict__ R,
-                                                              int compensated)
+                                          const float* __restrict__ P, QState c, float* __restrict__ R,
+                                          int compensated)
 {
     const int g = bx_ * blockDim.x + threadIdx.x;
     if (g >= d.F1) return;
@@ -957,7 +957,7 @@ struct k_gf_g {
 // gathers.  The edge's outputs land at its id e = e_out(x) - (V1 + F1).
 template <bool LAK, bool STATE, bool PQ, int BS, bool BND = false>
 __device__ __forceinline__ void k_g2_body(const unsigned bx_, FastDims d, Faces<PQ> pf, const int* __restrict__ ids,
-                                                              const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
+                                          const float* __restrict__ P, QState p, QState c, float* __restrict__ R)
 {
     const int x = bx_ * blockDim.x + threadIdx.x;
     const bool valid = x < d.N1;
@@ -1290,7 +1290,7 @@ __device__ __noinline__ void g3_warp_column(FastDims d, const float* __restrict_
 // columns k_g1 sums).
 template <bool LAK, bool STATE, int BS, bool BND = false, bool SG = false>
 __device__ __forceinline__ void k_g3_body(const unsigned bx_, FastDims d, const float* __restrict__ P, QState p, QState c,
-                                                              SlotScratch z, float* __restrict__ R, int compensated, int nv)
+                                          SlotScratch z, float* __restrict__ R, int compensated, int nv)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     if (STATE && v == nv) c.sptr[d.V] = d.N;
@@ -1357,8 +1357,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int pol
 
 template <bool LAK, bool STATE>
 __device__ __forceinline__ void k_g3_bulk_body(const unsigned bx_, FastDims d, const float* __restrict__ P, QState p,
-                                                                   QState c, SlotScratch z, float* __restrict__ R,
-                                                                   int compensated, int nv, DevStatus* st, int polls)
+                                               QState c, SlotScratch z, float* __restrict__ R,
+                                               int compensated, int nv, DevStatus* st, int polls)
 {
     __shared__ __align__(128) float4 zs[2 * kBulkSlots];
     __shared__ __align__(16) int rs[kBulkSlots + 8];

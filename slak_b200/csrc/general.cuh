@@ -32,7 +32,7 @@ enum : int { SF_OWNER = 1, SF_BOUT = 2, SF_BIN = 4 };
 // polygon levels: corner -> face (validating ptr) and the valences in one pass
 // over the faces
 __device__ __forceinline__ void k_face_map_valence_body(const unsigned bx_, const int* __restrict__ ptr, const int* __restrict__ ids, int F, int N, int V,
-                                                                            int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
+                                                        int* __restrict__ cface, int* __restrict__ cnt, DevStatus* st)
 {
     int f = bx_ * blockDim.x + threadIdx.x;
     if (f == 0 && (ptr[0] != 0 || ptr[F] != N)) set_error(st, 4, -1);
@@ -115,7 +115,7 @@ struct k_valence_hist_g {
 // vertex than its column counts: those find no slot (r < 0) and are dropped,
 // so nothing is written outside the column; the level fails with BAD_MESH.
 __device__ __forceinline__ void k_bucket_body(const unsigned bx_, const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
-                                                                  int* __restrict__ fill, int* __restrict__ loose)
+                                              int* __restrict__ fill, int* __restrict__ loose)
 {
     int c = bx_ * blockDim.x + threadIdx.x;
     if (c >= N) return;
@@ -157,8 +157,8 @@ __device__ __forceinline__ void vsort_neighbours(Faces<QUAD> fc, const int* __re
 
 template <bool QUAD>
 __device__ __forceinline__ void k_vsort_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
-                                                                 const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
-                                                                 int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
+                                             const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
+                                             int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -273,9 +273,9 @@ struct ColRegs {         // a column of at most 8 slots in registers
 // With `xtw` the twin of every corner is exported as well (corner -> twin).
 template <bool LAK>
 __device__ __forceinline__ void k_edges_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                                                                 const int* __restrict__ snext, const int* __restrict__ sprev,
-                                                                 const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
-                                                                 int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
+                                             const int* __restrict__ snext, const int* __restrict__ sprev,
+                                             const int* __restrict__ sprevc, int* __restrict__ stw, int* __restrict__ sflag,
+                                             int* __restrict__ ecnt, int* __restrict__ bcount, int* __restrict__ xtw, DevStatus* st)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -362,9 +362,9 @@ __device__ __forceinline__ void check_level(int v, const int* eptr, int V, int E
 }
 
 __device__ __forceinline__ void k_eids_slak_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                                                                     const int* __restrict__ stw, const int* __restrict__ sflag,
-                                                                     const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
-                                                                     int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
+                                                 const int* __restrict__ stw, const int* __restrict__ sflag,
+                                                 const int* __restrict__ eptr, int Ecap, int* __restrict__ eid,
+                                                 int2* __restrict__ H, DevStatus* st, const int* bcount, int B, int li)
 {
     int v = bx_ * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
@@ -501,10 +501,10 @@ __device__ __noinline__ void eids_lak_warp(const int* __restrict__ sc, const int
 // max->min), -1 where one is missing.  Columns longer than kBigCol go to
 // their warp.
 __device__ __forceinline__ void k_eids_lak_body(const unsigned bx_, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                                                                    const int* __restrict__ snext, const int* __restrict__ sprev,
-                                                                    const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
-                                                                    int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
-                                                                    int li)
+                                                const int* __restrict__ snext, const int* __restrict__ sprev,
+                                                const int* __restrict__ sprevc, const int* __restrict__ eptr, int Ecap,
+                                                int* __restrict__ eid, int2* __restrict__ H, DevStatus* st, const int* bcount, int B,
+                                                int li)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     check_level(v, eptr, V, Ecap, bcount, B, st, li);
@@ -544,9 +544,9 @@ struct k_eids_lak_g {
 // t[c] = slot[twin(prev c)], -1 where prev(c) has no twin.
 template <bool QUAD, bool LAK>
 __device__ __forceinline__ void k_refine_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, const int* __restrict__ eid, int N,
-                                                                  int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
-                                                                  int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
-                                                                  int* __restrict__ xt)
+                                              int V, int F, int4* __restrict__ out_ids, int* __restrict__ out_ptr,
+                                              int4* __restrict__ out_vals, const int* __restrict__ xslot, const int* __restrict__ xtw,
+                                              int* __restrict__ xt)
 {
     int c = bx_ * blockDim.x + threadIdx.x;
     if (c >= N) return;
@@ -588,7 +588,7 @@ struct k_refine_g {
 // SLAK quad face point: ((c0 + c2) + (c1 + c3)) * 1/4, the pairing of the
 // width-16 shuffles in calculateFaceEdgepointsQuad (CatmullClarkKernels.cuh:586-594)
 __device__ __forceinline__ void k_fp_slak_quad_body(const unsigned bx_, const int4* __restrict__ ids4, const float* __restrict__ P, int F,
-                                                                        float* __restrict__ FP)
+                                                    float* __restrict__ FP)
 {
     int f = bx_ * blockDim.x + threadIdx.x;
     if (f >= F) return;
@@ -617,7 +617,7 @@ struct k_fp_slak_quad_g {
 //         LAKCatmullClarkImpl.cu:175-178)
 template <bool QUAD, bool LAK>
 __device__ __forceinline__ void k_fp_seq_body(const unsigned bx_, const int* __restrict__ ptr, const int* __restrict__ ids, const float* __restrict__ P,
-                                                                  int F, float* __restrict__ FP)
+                                              int F, float* __restrict__ FP)
 {
     int f = bx_ * blockDim.x + threadIdx.x;
     if (f >= F) return;
@@ -651,7 +651,7 @@ struct k_fp_seq_g {
 // (calculateInternal/ExternalEdgepoints, LAKCatmullClarkKernels.cuh:437-462).
 template <bool QUAD, bool LAK>
 __device__ __forceinline__ void k_ep_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, const int2* __restrict__ H, int E,
-                                                              const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
+                                          const float* __restrict__ P, const float* __restrict__ FP, float* __restrict__ EP)
 {
     int e = bx_ * blockDim.x + threadIdx.x;
     if (e >= E) return;
@@ -781,9 +781,9 @@ __device__ __noinline__ void vp_slak_warp(Faces<QUAD> fc, const int* __restrict_
 // Columns longer than kBigCol go to their warp.
 template <bool QUAD>
 __device__ __forceinline__ void k_vp_slak_body(const unsigned bx_, Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                                                                   const int* __restrict__ snext, const int* __restrict__ sprev,
-                                                                   const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
-                                                                   const float* __restrict__ FP, float* __restrict__ R, int compensated)
+                                               const int* __restrict__ snext, const int* __restrict__ sprev,
+                                               const int* __restrict__ sflag, int boundary, const float* __restrict__ P,
+                                               const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     const bool valid = v < V;
@@ -954,10 +954,10 @@ __device__ __noinline__ void vp_lak_warp(Faces<QUAD> fc, const int* __restrict__
 // Columns longer than kBigCol go to their warp.
 template <bool QUAD>
 __device__ __forceinline__ void k_vp_lak_body(const unsigned bx_, Faces<QUAD> fc, int V, const int* __restrict__ sptr, const int* __restrict__ sc,
-                                                                  const int* __restrict__ snext, const int* __restrict__ sprev,
-                                                                  const int* __restrict__ sprevc, const int* __restrict__ sflag,
-                                                                  const int* __restrict__ eid, int boundary, const float* __restrict__ P,
-                                                                  const float* __restrict__ FP, float* __restrict__ R, int compensated)
+                                              const int* __restrict__ snext, const int* __restrict__ sprev,
+                                              const int* __restrict__ sprevc, const int* __restrict__ sflag,
+                                              const int* __restrict__ eid, int boundary, const float* __restrict__ P,
+                                              const float* __restrict__ FP, float* __restrict__ R, int compensated)
 {
     const int v = bx_ * blockDim.x + threadIdx.x;
     const bool valid = v < V;

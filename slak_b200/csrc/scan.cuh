@@ -105,7 +105,7 @@ struct k_scan_tiles_g {
 };
 
 __device__ __forceinline__ void k_scan_final_body(const unsigned bx_, const int* __restrict__ in, int64_t n,
-                                                                      const int* __restrict__ tsum, int nt, int* __restrict__ out)
+                                                  const int* __restrict__ tsum, int nt, int* __restrict__ out)
 {
     __shared__ int tile[kScanTile];
     __shared__ int tot;
@@ -153,8 +153,8 @@ struct k_scan_final_g {
 constexpr int kScanSmallTiles = 2048;
 
 __device__ __forceinline__ void k_scan_final_small_body(const unsigned bx_, const int* __restrict__ in, int64_t n,
-                                                                            const int* __restrict__ tsum, int nt,
-                                                                            int* __restrict__ out)
+                                                        const int* __restrict__ tsum, int nt,
+                                                        int* __restrict__ out)
 {
     __shared__ int tile[kScanTile];
     __shared__ int tot;

@@ -293,19 +293,19 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
         launch_g<k_vsort_g<true>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
-                                                       s.sprevc, xslot);
+                                  s.sprevc, xslot);
     } else {
         Faces<false> fc{L.ptr, s.cface};
         launch_g<k_vsort_g<false>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
-                                                        s.sprevc, xslot);
+                                   s.sprevc, xslot);
     }
     lc.after("k_vsort");
     if (scheme == SLAK_SCHEME_LAK)
         launch_g<k_edges_g<true>>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
-                                                        s.sflag, s.ecnt, bcount, xtw, st);
+                                  s.sflag, s.ecnt, bcount, xtw, st);
     else
         launch_g<k_edges_g<false>>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.stw,
-                                                         s.sflag, s.ecnt, bcount, xtw, st);
+                                   s.sflag, s.ecnt, bcount, xtw, st);
     lc.after("k_edges");
     scan_exclusive(s.ecnt, s.eptr, V, s.tmp, str, &dummy);
     lc.after("scan(edges)", 3);
@@ -325,10 +325,10 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     const int* bcount = &st->bcount[li];
     if (lak)
         launch_g<k_eids_lak_g>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.eptr, E, s.eid,
-                                                     s.H, st, bcount, (int)L.B, li);
+                               s.H, st, bcount, (int)L.B, li);
     else
         launch_g<k_eids_slak_g>(grid_for(V), kBlock, str, V, s.sptr, s.sc, s.stw, s.sflag, s.eptr, E, s.eid, s.H, st,
-                                                      bcount, (int)L.B, li);
+                                bcount, (int)L.B, li);
     lc.after("k_eids");
     // the refined quads (side stream 0) need only the edge ids; the positions
     // (k_fp, then k_ep on side stream 1 beside k_vp) need the face points
@@ -336,13 +336,13 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     cudaStream_t s_ref = lc.conc ? lc.side[0] : str;
     if (lak)
         launch_g<k_refine_g<QUAD, true>>(grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
-                                                                reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
-                                                                reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
-                                                                nullptr);
+                                         reinterpret_cast<int4*>(L.o_ids), L.o_ptr,
+                                         reinterpret_cast<int4*>(L.o_vals), nullptr, nullptr,
+                                         nullptr);
     else
         launch_g<k_refine_g<QUAD, false>>(grid_for(N), kBlock, s_ref, fc, L.ids, s.eid, N, V, F,
-                                                                 reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
-                                                                 s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
+                                          reinterpret_cast<int4*>(L.o_ids), nullptr, nullptr,
+                                          s.xslot, s.xtw, L.export_state ? s.xt : nullptr);
     lc.after("k_refine");
     float* R = L.o_verts;
     float* FPo = R + 4 * (size_t)V;
@@ -364,10 +364,10 @@ void launch_rest(const Level& L, int li, int scheme, bool compensated, Scratch& 
     const int bnd = L.B > 0;
     if (lak)
         launch_g<k_vp_lak_g<QUAD>>(grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sprevc, s.sflag,
-                                                        s.eid, bnd, L.verts, FPo, R, compensated);
+                                   s.eid, bnd, L.verts, FPo, R, compensated);
     else
         launch_g<k_vp_slak_g<QUAD>>(grid_for(V), kBlock, str, fc, V, s.sptr, s.sc, s.snext, s.sprev, s.sflag, bnd,
-                                                         L.verts, FPo, R, compensated);
+                                    L.verts, FPo, R, compensated);
     lc.after("k_vp");
     if (lc.conc) { lc.join(0); lc.join(1); }
 }
