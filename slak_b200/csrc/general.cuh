@@ -140,10 +140,11 @@ struct k_bucket_g {
 };
 
 // Each column sorted by corner index: a corner's slot is the number of smaller
-// corners in its column (corner indices are distinct).  Columns of up to 8 are
-// ranked by their own thread in registers; a longer column (a high-valence
-// vertex) is ranked by its warp, one corner per lane.  With `xslot` the slot of
-// every corner is exported as well (corner -> slot, for the fast path).
+// corners in its column (corner indices are distinct).  One thread per corner
+// (four times the threads of one per vertex, and the corner-indexed reads and
+// writes coalesced); a column of up to 8 is read into registers at once.  With
+// `xslot` the slot of every corner is exported as well (corner -> slot, for
+// the fast path).
 template <bool QUAD>
 __device__ __forceinline__ void vsort_neighbours(Faces<QUAD> fc, const int* __restrict__ ids, int s, int c,
                                                  int* __restrict__ snext, int* __restrict__ sprev,
@@ -156,52 +157,41 @@ __device__ __forceinline__ void vsort_neighbours(Faces<QUAD> fc, const int* __re
 }
 
 template <bool QUAD>
-__device__ __forceinline__ void k_vsort_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
-                                             const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
-                                             int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
+__device__ __forceinline__ void k_vsort_body(const unsigned bx_, Faces<QUAD> fc, const int* __restrict__ ids, int N,
+                                             int V, const int* __restrict__ sptr, const int* __restrict__ loose,
+                                             int* __restrict__ sc, int* __restrict__ snext, int* __restrict__ sprev,
+                                             int* __restrict__ sprevc, int* __restrict__ xslot)
 {
-    const int v = bx_ * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    int b = 0, n = 0;
-    if (v < V) { b = sptr[v]; n = sptr[v + 1] - b; }
-    if (v < V && n <= 8) {
+    // one thread per corner c: its slot is its rank by corner id within its
+    // vertex's column (the column's entries are distinct corner ids)
+    const int c = bx_ * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    const int v = __ldg(ids + c);
+    if ((unsigned)v >= (unsigned)V) return;              // flagged by the valence pass
+    const int b = __ldg(sptr + v), n = __ldg(sptr + v + 1) - b;
+    int r = 0;
+    if (n <= 8) {
         int u[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) u[k] = k < n ? __ldg(loose + b + k) : INT32_MAX;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            int r = 0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) r += u[j] < u[k];
-            if (k < n) {
-                sc[b + r] = u[k];
-                if (xslot) xslot[u[k]] = b + r;
-                vsort_neighbours(fc, ids, b + r, u[k], snext, sprev, sprevc);
-            }
-        }
+        for (int k = 0; k < 8; ++k) r += u[k] < c;
+    } else {
+        for (int j = 0; j < n; ++j) r += __ldg(loose + b + j) < c;
     }
-    unsigned big = __ballot_sync(0xffffffffu, v < V && n > 8);
-    while (big) {
-        const int src = __ffs(big) - 1;
-        big &= big - 1;
-        const int bb = __shfl_sync(0xffffffffu, b, src), bn = __shfl_sync(0xffffffffu, n, src);
-        for (int k = lane; k < bn; k += 32) {
-            const int x = __ldg(loose + bb + k);
-            int r = 0;
-            for (int j = 0; j < bn; ++j) r += __ldg(loose + bb + j) < x;
-            sc[bb + r] = x;
-            if (xslot) xslot[x] = bb + r;
-            vsort_neighbours(fc, ids, bb + r, x, snext, sprev, sprevc);
-        }
-    }
+    // a malformed mesh's dropped corner is not in its column: no slot
+    if (r >= n) return;
+    sc[b + r] = c;
+    if (xslot) xslot[c] = b + r;
+    vsort_neighbours(fc, ids, b + r, c, snext, sprev, sprevc);
 }
 template <bool QUAD>
-__global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int V, const int* __restrict__ sptr,
+__global__ void k_vsort(Faces<QUAD> fc, const int* __restrict__ ids, int N, int V, const int* __restrict__ sptr,
                         const int* __restrict__ loose, int* __restrict__ sc, int* __restrict__ snext,
                         int* __restrict__ sprev, int* __restrict__ sprevc, int* __restrict__ xslot)
 {
     griddep_enter();
-    k_vsort_body<QUAD>(blockIdx.x, fc, ids, V, sptr, loose, sc, snext, sprev, sprevc, xslot);
+    k_vsort_body<QUAD>(blockIdx.x, fc, ids, N, V, sptr, loose, sc, snext, sprev, sprevc, xslot);
 }
 template <bool QUAD>
 struct k_vsort_g {

@@ -292,11 +292,11 @@ void launch_topology_a(const Level& L, int li, int scheme, Scratch& s, DevStatus
     int* xtw = L.export_state ? s.xtw : nullptr;
     if (L.quad) {
         Faces<true> fc{L.ptr, s.cface};
-        launch_g<k_vsort_g<true>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_g<k_vsort_g<true>>(grid_for(N), kBlock, str, fc, L.ids, N, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                   s.sprevc, xslot);
     } else {
         Faces<false> fc{L.ptr, s.cface};
-        launch_g<k_vsort_g<false>>(grid_for(V), kBlock, str, fc, L.ids, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
+        launch_g<k_vsort_g<false>>(grid_for(N), kBlock, str, fc, L.ids, N, V, s.sptr, s.sflag, s.sc, s.snext, s.sprev,
                                    s.sprevc, xslot);
     }
     lc.after("k_vsort");
