@@ -60,31 +60,67 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """SM clock and clock-event (throttle) samples while the timed region runs.
+
+    Reads NVML directly every 2 ms (the device found by its UUID, so
+    CUDA_VISIBLE_DEVICES does not matter), which gives tens of samples even in
+    a region of ~12 ms; without NVML it falls back to nvidia-smi every 200 ms.
+    Only reads: nothing here changes a GPU setting."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []          # (sm MHz, max sm MHz, set of reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        self._handle = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            self._handle = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self._nvml = pynvml
+            self._bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                          pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        except Exception:
+            self._nvml = None
 
-    def _run(self):
+    def _run_nvml(self):
+        n, h = self._nvml, self._handle
+        mx = float(n.nvmlDeviceGetMaxClockInfo(h, n.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            try:
+                sm = float(n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM))
+                r = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, mx, {self.NAMES[i] for i, bit in enumerate(self._bits) if r & bit}))
+            except Exception:
+                pass
+            self._stop.wait(0.002)
+
+    def _run_smi(self):
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True,
                                      timeout=5).stdout.strip()
                 if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
+                    r = [x.strip() for x in out.split(",")]
+                    if r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                        self.rows.append((float(r[1]), float(r[2]),
+                                          {self.NAMES[i] for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"}))
             except Exception:
                 pass
             self._stop.wait(0.2)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+        self.source = "nvml" if self._nvml is not None else "nvidia-smi"
+        self._t = threading.Thread(target=self._run_nvml if self._nvml is not None else self._run_smi, daemon=True)
         self._t.start()
         return self
 
@@ -94,13 +130,11 @@ class ClockSampler:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0, "source": self.source}
+        sm = [r[0] for r in self.rows]
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(set().union(*[r[2] for r in self.rows])), "samples": len(self.rows),
+                "source": self.source}
 
 
 def _dist():
