@@ -14,8 +14,9 @@ One step = one full multi-level subdivision of that mesh.
           the other scheme, the capped cylinder (7 levels, both schemes), the
           32x32 torus and the icosphere
   batched the 2,000-mesh batch as one CUDA graph beside the per-mesh loop of
-          plans and the per-mesh loop of slak_subdivide (--no-extras skips
-          these two blocks)
+          plans and the per-mesh loop of slak_subdivide
+  batched_small  2,000 small meshes, grouped launches against chains
+          (--no-extras skips secondary, batched and batched_small)
 
 --impl reference times the reference's own CUDA path (GPUPeople/SLAK compiled
 from its sources for sm_100a, oracle/_ref) on the same workload.
@@ -348,7 +349,58 @@ def run_ours(args, dist, rank, ws):
         b = run_batch(args, torch, dist, rank, ws)
         b.pop("clocks", None)
         out["batched"] = b
+        out["batched_small"] = run_small_batch(args, torch)
     return out
+
+
+def run_small_batch(args, torch, count=2000, fmax=2000):
+    """A batch of many small meshes (faces log-uniform in [100, fmax], levels
+    1-4), where launches rather than bytes bound the time: grouped launches
+    (the default) against every mesh in chains (SLAK_BATCH_GROUP_QUADS=0), one
+    CUDA graph each, median device time of 7 executions."""
+    from slak_b200 import _abi, api, meshgen
+    from slak_b200.mesh import LAK, SLAK
+    scheme = SLAK if args.scheme == "slak" else LAK
+    items = [(meshgen.batch_mesh(it), it.levels) for it in meshgen.batch_specs(count, seed=5, fmin=100, fmax=fmax)]
+    if scheme == LAK:
+        items = [(m if m.ptr is not None else m.with_quad_ptr(), l) for m, l in items]
+    dms = [api.DeviceMesh.from_host(m) for m, _ in items]
+    stream = torch.cuda.Stream()
+    res = {"meshes": count, "faces": f"log-uniform in [100, {fmax}]", "levels": "uniform in 1..4"}
+    saved = os.environ.get("SLAK_BATCH_GROUP_QUADS")
+    try:
+        for name, gq in (("grouped", saved), ("chains", "0")):
+            if gq is None:
+                os.environ.pop("SLAK_BATCH_GROUP_QUADS", None)
+            else:
+                os.environ["SLAK_BATCH_GROUP_QUADS"] = gq
+            with torch.cuda.stream(stream):
+                b = api.Batch(dms, [l for _, l in items], scheme, _abi.PLAN_GRAPH, stream=stream)
+                for _ in range(3):
+                    b.execute(stream)
+                b.check(stream)
+                ms = []
+                for _ in range(7):
+                    a = torch.cuda.Event(enable_timing=True)
+                    c = torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    b.execute(stream)
+                    c.record(stream)
+                    c.synchronize()
+                    ms.append(a.elapsed_time(c))
+                b.check(stream)
+                res[f"{name}_ms"] = statistics.median(ms)
+                res[f"{name}_launches"] = b.launches
+                res[f"{name}_groups"] = b.groups
+                b.close()
+    finally:
+        if saved is None:
+            os.environ.pop("SLAK_BATCH_GROUP_QUADS", None)
+        else:
+            os.environ["SLAK_BATCH_GROUP_QUADS"] = saved
+    res["refined_faces"] = int(sum(m.nnz * 4 ** (l - 1) for m, l in items))
+    res["speedup_grouped_vs_chains"] = res["chains_ms"] / res["grouped_ms"]
+    return res
 
 
 def plan_time(mesh, levels, scheme, steps, warmup, stream, torch, flush):
